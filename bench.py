@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 SIMPLE solver.
+
+Workload: the reference's default case as its README states it:
+a 2D channel of 512 x 128 cells on [-0.0625, 0.0625] x [-0.0125, 0.0125],
+water (rho 998.2, mu 1.002e-3), west inlet 0.001 m/s, east outlet, no-slip
+north/south walls, SIMPLE with alpha_u 0.75 / alpha_p 0.25 and 10/10/20
+red-black Gauss-Seidel sweeps per outer iteration, FP32.  Inputs are
+synthetic: the flow starts from rest and is advanced by the warm-up steps.
+
+One step = OUTER_PER_STEP SIMPLE outer iterations (fixed work: the
+convergence test runs but does not stop the loop).  The metric is
+cell-updates/s, one cell-update being one relaxed point update of one unknown
+(u, v or p') at one cell.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs an independent
+replica: the plain solve does not shard (one grid per GPU), so the scaling is
+weak and `value` sums all ranks' cell-updates over the slowest rank's time.
+
+--impl reference times the reference's own implementation of this workload:
+its CUDA build (oracle/_ref/, compiled from the reference's sources with the
+same case written into its config.h) when present, else the serial CPU
+restatement of its kernels.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "incompflow-cuda_b200", "python"))
+
+WORKLOAD = "channel2d_512x128"
+OUTER_PER_STEP = 100
+BYTES_PER_UPDATE_2D = 32      # stored-coefficient GS update, FP32: 4*(2*dim+4)
+METRIC = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def workload_cfg():
+    import ifc
+
+    return ifc.channel2d(512, 128)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(seconds: float):
+    """The serial CPU restatement of the reference's kernels (oracle, FP32,
+    1 core) on a bounded sample of the same workload: outer iterations from
+    rest until `seconds` of CPU time have passed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    from helpers import to_oracle_cfg
+
+    cfg = to_oracle_cfg(workload_cfg())
+    o = O.Oracle(cfg, "f")
+    t0 = time.perf_counter()
+    its, updates = 0, 0
+    while time.perf_counter() - t0 < seconds:
+        nm = o.outer_iteration()
+        its += 1
+        updates += o.N * (nm["sweeps"][0] + nm["sweeps"][1] + nm["sweeps"][3])
+    dt = time.perf_counter() - t0
+    return {"value": updates / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{its} outer iterations of {WORKLOAD} from rest, serial C oracle (FP32, red-black GS), "
+                      f"{dt:.1f} s"}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import ifc
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    cfg = workload_cfg()
+    cfg["stream"] = stream.cuda_stream
+    s = ifc.Solver(cfg)
+    N = s.N
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        s.iterate(OUTER_PER_STEP)
+    # Device-resident throughput: K steps, each timed with CUDA events on the
+    # solver's stream; the L2 is flushed between steps (outside the events).
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    updates, launches = 0, 0
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        ev[k][0].record(stream)
+        st = s.iterate(OUTER_PER_STEP)
+        ev[k][1].record(stream)
+        updates += st["cell_updates"]
+        launches += st["kernel_launches"]
+    barrier()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # End to end through the public C ABI with host buffers: every step
+    # uploads u, v, p from pinned host memory, runs the step, reads them back.
+    host_in = {k: torch.from_numpy(s.get(k)).pin_memory() for k in ("u", "v", "p")}
+    host_out = {k: torch.empty_like(v).pin_memory() for k, v in host_in.items()}
+    lib = ifc.load()
+    fid = {k: ifc.FIELDS.index(k) for k in host_in}
+    nbytes = N * 4
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e2e_updates = 0
+    barrier()
+    for k in range(args.steps):
+        e2e_ev[k][0].record(stream)
+        for name, t in host_in.items():
+            assert lib.ifc_set_field(s._h, fid[name], C.c_void_p(t.data_ptr()), nbytes) == 0
+        st = s.iterate(OUTER_PER_STEP)
+        for name, t in host_out.items():
+            assert lib.ifc_get_field(s._h, fid[name], C.c_void_p(t.data_ptr()), nbytes) == 0
+        e2e_ev[k][1].record(stream)
+        e2e_updates += st["cell_updates"]
+    barrier()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+
+    # Roofline of the dominant kernel sequence: the p' sweeps (largest share of
+    # the launch list), timed alone with CUDA events on the solver's stream.
+    stage_ms, stage_launches = s.time_stage("pcorr_solve", reps=50)
+    n_p = cfg["nIter_p"]
+    alg_bytes = n_p * BYTES_PER_UPDATE_2D * N
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+
+    t_max = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    tot = torch.tensor([float(updates), float(e2e_updates)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    ms_all, e2e_all = t_max.tolist()
+    upd_all, e2e_upd_all = tot.tolist()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_seconds)
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": upd_all / (ms_all * 1e-3),
+            "unit": METRIC,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_all / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic: flow from rest, advanced by the warm-up steps",
+            "config": {"workload": WORKLOAD, "nx": 512, "ny": 128, "outer_iterations_per_step": OUTER_PER_STEP,
+                       "sweeps_u_v_p": [cfg["nIter_u"], cfg["nIter_v"], cfg["nIter_p"]],
+                       "linear_solver": "red-black Gauss-Seidel", "precision": "fp32 sweeps, fp64 norms",
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_upd_all / (e2e_all * 1e-3), "unit": METRIC,
+                    "h2d_bytes_per_step": 3 * nbytes, "d2h_bytes_per_step": 3 * nbytes},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "p' red-black sweeps (pcorr_solve stage)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": alg_bytes / max(stage_launches, 1),
+                         "launches_per_stage": stage_launches, "stage_ms": stage_ms,
+                         "note": "working set fits in L2 (126 MB); ref-equivalent bytes"},
+            "ref_equivalent_gbs": upd_all / (ms_all * 1e-3) * BYTES_PER_UPDATE_2D / 1e9,
+            "clocks": clk,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_bench_channel512x128")
+    if os.path.exists(ref_bin):
+        out = subprocess.run([ref_bin, str(args.warmup), str(args.steps)], capture_output=True, text=True,
+                             timeout=1800)
+        if out.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build exited {out.returncode}"}))
+            return
+        rec = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+        cfg = workload_cfg()
+        N = 512 * 128
+        upd = N * (cfg["nIter_u"] + cfg["nIter_v"] + cfg["nIter_p"]) * rec["outer_per_step"]
+        step_ms = rec["step_ms"]
+        value = upd * len(step_ms) / (sum(step_ms) * 1e-3)
+        kind, cores = "reference", 1
+        sample = (f"reference CUDA build (src/Solver.cu + include/kernels.cuh, -O2, sm_100a), "
+                  f"{rec['outer_per_step']} outer iterations per Solver::solve() call")
+        ms_per_step = statistics.mean(step_ms)
+    else:
+        cpu = cpu_baseline(args.cpu_seconds)
+        value = cpu["value"]
+        kind, cores, sample = "port", 1, cpu["sample"]
+        N = 512 * 128
+        ms_per_step = OUTER_PER_STEP * 40 * N / value * 1e3
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: flow from rest",
+        "config": {"workload": WORKLOAD, "nx": 512, "ny": 128, "outer_iterations_per_step": OUTER_PER_STEP},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+/*
+ * ifc.h -- C ABI of the B200 SIMPLE solver (libifc.so).
+ *
+ * The reference (WanZijun271/IncompFlow-CUDA) exposes one C++ class, Solver
+ * (include/Solver.h:8-72), configured at compile time by include/config.h.
+ * This header is the plain-C boundary underneath a drop-in replacement of that
+ * class (incompflow-cuda_b200/host/Solver.h): opaque handles, int status codes,
+ * host pointers and sizes only, no exceptions and no C++ or torch types.
+ *
+ * Ownership: the library owns all device memory of a handle; the caller owns
+ * every host buffer it passes.  Threading: one handle per host thread; calls on
+ * one handle must not overlap.  All work of a handle runs on one CUDA stream
+ * (its own, or ifc_config.stream).  Every call that returns data is
+ * host-synchronous on return, as the reference's Solver methods are.
+ */
+#ifndef IFC_H
+#define IFC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFC_ABI_VERSION 1
+
+/* Status codes returned by every entry point (the reference reports none, D11). */
+typedef enum ifc_status {
+    IFC_OK = 0,
+    IFC_NOT_CONVERGED = 1,   /* num_outer_iter reached without convergence */
+    IFC_DIVERGED = 2,        /* NaN/Inf in a norm, or a norm grew 1e6x over its running max */
+    IFC_TIMEOUT = 3,         /* a bounded device wait gave up */
+    IFC_CUDA_ERROR = 4,
+    IFC_BAD_CONFIG = 5,
+    IFC_BAD_ARGUMENT = 6,
+    IFC_IO_ERROR = 7,
+    IFC_UNSUPPORTED = 8
+} ifc_status;
+
+/* Boundary faces and types: include/constants.h:7-12 and :32-34. */
+enum { IFC_EAST = 0, IFC_WEST = 1, IFC_NORTH = 2, IFC_SOUTH = 3, IFC_TOP = 4, IFC_BOTTOM = 5 };
+enum { IFC_WALL = 0, IFC_INLET = 1, IFC_OUTLET = 2 };
+
+enum { IFC_FP32 = 0, IFC_FP64 = 1 };
+/* Linear sweeps (reference: src/Solver.cu:868-966).  Gauss-Seidel runs in
+ * red-black order (deterministic); Jacobi ping-pongs two buffers. */
+enum { IFC_GAUSS_SEIDEL = 0, IFC_JACOBI = 1 };
+/* Convergence rule.  REFERENCE reproduces src/Solver.cu:237-268 exactly,
+ * including the division of every norm by the running max of the pressure norm;
+ * PER_FIELD divides each norm by its own running max (FP64). */
+enum { IFC_CRIT_REFERENCE = 0, IFC_CRIT_PER_FIELD = 1 };
+
+/* Field ids for ifc_get_field / ifc_set_field / ifc_device_ptr.  Layouts follow
+ * the reference: cells i + nx*(j + ny*k); uf i + (nx+1)*(j + ny*k);
+ * vf i + nx*(j + (ny+1)*k); wf i + nx*(j + ny*k) with k in [0, nz].
+ * IFC_FIELD_MOM_COEF / PCORR_COEF hold 2*dim+1 planes coef[cell + N*slot], slot
+ * order aC,aE,aW,aN,aS,aT,aB (include/constants.h:14-20); they are filled by
+ * ifc_run_stage(IFC_STAGE_MOM_ASSEMBLE / IFC_STAGE_PCORR_COEF), the fused
+ * solver never stores them. */
+enum {
+    IFC_FIELD_U = 0, IFC_FIELD_V, IFC_FIELD_W, IFC_FIELD_P, IFC_FIELD_T, IFC_FIELD_PCORR,
+    IFC_FIELD_UF, IFC_FIELD_VF, IFC_FIELD_WF, IFC_FIELD_MOM_AC,
+    IFC_FIELD_MOM_COEF, IFC_FIELD_PCORR_COEF,
+    IFC_FIELD_SRC_U, IFC_FIELD_SRC_V, IFC_FIELD_SRC_W, IFC_FIELD_SRC_P,
+    IFC_FIELD_COUNT
+};
+
+/* Every parameter of include/config.h:6-81 under the same meaning, plus the
+ * new-build additions at the end.  Values are doubles and are rounded to the
+ * solver's scalar type exactly as the reference's `constexpr scalar` are. */
+typedef struct ifc_config {
+    int dim;                          /* 2 or 3 */
+    int nx, ny, nz;                   /* nz is forced to 1 when dim == 2 */
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double thermal_conductivity;      /* carried for the VTK/config surface; the */
+    double specific_heat_capacity;    /* energy equation is not solved (as in the reference) */
+    double density;
+    double dynamic_viscosity;
+    int vel_bc_type[6];               /* velBCs::type, face order E W N S T B */
+    double vel_bc_val[6][3];          /* velBCs::val[face][u,v,w] */
+    int temp_bc_type[6];              /* TempBCs (carried, unused) */
+    double temp_bc_val[6];
+    int num_outer_iter;
+    int n_iter_u, n_iter_v, n_iter_w, n_iter_p;
+    double relax_u, relax_v, relax_w, relax_p;
+    double tol_u, tol_v, tol_w, tol_p, tol_mass;
+    /* ---- additions ---- */
+    int precision;                    /* IFC_FP32 (default) or IFC_FP64 */
+    int linear_solver;                /* IFC_GAUSS_SEIDEL (default) or IFC_JACOBI */
+    int criterion;                    /* IFC_CRIT_PER_FIELD (default) or IFC_CRIT_REFERENCE */
+    int pin_pressure;                 /* -1 auto (closed domains), 0 off, 1 on */
+    int sweeps_per_pass;              /* sweeps fused per device pass; 0 = tuned default */
+    int log_level;                    /* 0 silent, 1 reference log cadence on stdout */
+    const double *inlet_profile;      /* optional west-face inlet velocity per boundary cell (ny*nz) */
+    void *stream;                     /* cudaStream_t to run on, or NULL for a private stream */
+} ifc_config;
+
+typedef struct ifc_stats {
+    int status;                       /* ifc_status of the call */
+    int outer_iterations;             /* total outer iterations done by the handle */
+    int converged;
+    int sweeps[4];                    /* u v w p' sweeps in the last outer iteration */
+    long long cell_updates;           /* relaxed point updates done by the call */
+    double norm_p, norm_u, norm_v, norm_w, norm_uf, norm_vf, norm_wf, norm_mass;   /* RMS, FP64 */
+    double rel_p, rel_u, rel_v, rel_w, rel_uf, rel_vf, rel_wf;
+    double device_ms;                 /* device time of the call (CUDA events) */
+    long long kernel_launches;        /* device kernels launched by the call */
+} ifc_stats;
+
+typedef struct ifc_solver ifc_solver;
+
+/* Fill *cfg with the values of the reference's shipped include/config.h. */
+int ifc_config_default(ifc_config *cfg);
+
+/* Validate a config without touching the GPU. */
+int ifc_config_check(const ifc_config *cfg);
+
+/* Replaces Solver::Solver (src/Solver.cu:13-104): allocates every device
+ * buffer and sets uniform initial fields u=v=w=p=0, T=273 (the reference's
+ * default arguments, include/Solver.h:50). */
+int ifc_create(const ifc_config *cfg, ifc_solver **out);
+
+/* Replaces Solver::~Solver (src/Solver.cu:106-151). NULL is accepted. */
+int ifc_destroy(ifc_solver *h);
+
+/* The constructor's uniform initial values (src/Solver.cu:15-21); also resets
+ * face velocities, the iteration counter and the running norm maxima. */
+int ifc_set_uniform(ifc_solver *h, double u, double v, double w, double p, double temp);
+
+/* Copy a field between host and device.  bytes must equal the field's size in
+ * the handle's precision (ifc_field_size). */
+int ifc_set_field(ifc_solver *h, int field, const void *host, size_t bytes);
+int ifc_get_field(ifc_solver *h, int field, void *host, size_t bytes);
+size_t ifc_field_size(const ifc_solver *h, int field);
+
+/* Device address of a field (valid until ifc_destroy). */
+int ifc_device_ptr(ifc_solver *h, int field, void **dptr);
+
+/* Replaces Solver::solve (src/Solver.cu:153-299): SIMPLE outer iterations from
+ * the current state until convergence or num_outer_iter further iterations.
+ * The whole loop runs on the device (CUDA graph with a device-side convergence
+ * test); returns IFC_OK, IFC_NOT_CONVERGED or an error. */
+int ifc_solve(ifc_solver *h, ifc_stats *stats);
+
+/* Exactly n_outer outer iterations with the convergence test evaluated but not
+ * acted on (fixed work, for throughput measurement). */
+int ifc_iterate(ifc_solver *h, int n_outer, ifc_stats *stats);
+
+/* Replaces Solver::writeVTK (src/Solver.cu:301-367): ASCII RECTILINEAR_GRID,
+ * same header, coordinates and FIELD blocks, 6-significant-digit values.
+ * The path is used as given (the Solver wrapper prepends output/). */
+int ifc_write_vtk(ifc_solver *h, const char *path);
+
+/* The same writer on host arrays (no GPU needed); arrays are float for
+ * IFC_FP32 and double for IFC_FP64, nx*ny*nz each. */
+int ifc_write_vtk_host(const ifc_config *cfg, const void *u, const void *v, const void *w,
+                       const void *p, const void *temp, const char *path);
+
+/* ---- single steps, for testing one application of each device kernel ---- */
+enum {
+    IFC_STAGE_FACE_BC = 0,       /* first iteration: face init; then face BCs (kernels.cuh:10-95) */
+    IFC_STAGE_MOM_ASSEMBLE = 1,  /* materialise coefficients + sources (kernels.cuh:97-334) */
+    IFC_STAGE_MOM_SOLVE = 2,     /* assembly fused with the u,v,w sweeps (kernels.cuh:926-1005) */
+    IFC_STAGE_RHIE_CHOW = 3,     /* faces + face BCs + p' source + mass norm (kernels.cuh:336-500,542-581) */
+    IFC_STAGE_PCORR_COEF = 4,    /* materialise p' link coefficients (kernels.cuh:502-540) */
+    IFC_STAGE_PCORR_SOLVE = 5,   /* p' = 0, then the p' sweeps (src/Solver.cu:193-196) */
+    IFC_STAGE_UPDATE = 6,        /* corrections, norms, convergence test (kernels.cuh:583-843) */
+    IFC_STAGE_COUNT = 7
+};
+int ifc_run_stage(ifc_solver *h, int stage);
+
+/* n sweeps of one equation (0=u 1=v 2=w 3=p') with the coefficients and
+ * sources currently materialised by IFC_STAGE_MOM_ASSEMBLE / PCORR_COEF;
+ * sq_norms (optional, n entries) receives sum (d phi)^2 of each sweep. */
+int ifc_sweep(ifc_solver *h, int eq, int n, double *sq_norms);
+
+/* Average device time (ms, CUDA events on the handle's stream) of one launch
+ * sequence of a stage, over reps back-to-back repetitions on the current state;
+ * *launches receives the kernels one repetition launches.  For profiling. */
+int ifc_time_stage(ifc_solver *h, int stage, int reps, double *ms, int *launches);
+
+/* Norms of the last outer iteration and the running maxima (see ifc_stats). */
+int ifc_get_stats(ifc_solver *h, ifc_stats *stats);
+
+const char *ifc_status_string(int status);
+const char *ifc_last_error(const ifc_solver *h);
+int ifc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,639 @@
+// ifc_engine.cuh -- host-side engine of one solver handle: device buffers, the
+// SIMPLE outer iteration as a CUDA graph with a device-side loop condition
+// (conditional WHILE node), single-step launches for testing, and host
+// transfers.  Replaces the reference's Solver members (src/Solver.cu:13-966).
+#pragma once
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ifc.h"
+#include "ifc_kernels.cuh"
+#include "ifc_fused2d.cuh"
+
+namespace ifc {
+
+struct EngineBase {
+    virtual ~EngineBase() {}
+    virtual int set_uniform(double u, double v, double w, double p, double t) = 0;
+    virtual int set_field(int field, const void *host, size_t bytes) = 0;
+    virtual int get_field(int field, void *host, size_t bytes) = 0;
+    virtual size_t field_size(int field) const = 0;
+    virtual void *device_ptr(int field) = 0;
+    virtual int run(int n_outer, int act, ifc_stats *st) = 0;
+    virtual int run_stage(int stage) = 0;
+    virtual int sweep(int eq, int n, double *sq) = 0;
+    virtual int stats(ifc_stats *st) = 0;
+    virtual int time_stage(int stage, int reps, double *ms, int *launches) = 0;
+    std::string err;
+};
+
+#define IFC_CK(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+            return IFC_CUDA_ERROR;                                                        \
+        }                                                                                 \
+    } while (0)
+
+// Geometry and constants in the scalar type, evaluated like the reference's
+// constexpr expressions (include/constants.h:22-28, include/config.h).
+template <typename T>
+Params<T> make_params(const ifc_config &c)
+{
+    Params<T> P;
+    std::memset(&P, 0, sizeof(P));
+    Geo<T> &g = P.g;
+    g.dim = c.dim;
+    g.nx = c.nx;
+    g.ny = c.ny;
+    g.nz = c.dim == 2 ? 1 : c.nz;
+    g.N = g.nx * g.ny * g.nz;
+    const T xmax = (T)c.xmax, xmin = (T)c.xmin, ymax = (T)c.ymax, ymin = (T)c.ymin;
+    const T zmax = (T)c.zmax, zmin = (T)c.zmin;
+    g.dx = (xmax - xmin) / (T)g.nx;
+    g.dy = (ymax - ymin) / (T)g.ny;
+    g.dz = (zmax - zmin) / (T)g.nz;
+    g.Ax = g.dy * g.dz;
+    g.Ay = g.dz * g.dx;
+    g.Az = g.dx * g.dy;
+    g.rho = (T)c.density;
+    g.mu = (T)c.dynamic_viscosity;
+    const double rl[4] = {c.relax_u, c.relax_v, c.relax_w, c.relax_p};
+    const double tl[4] = {c.tol_u, c.tol_v, c.tol_w, c.tol_p};
+    for (int q = 0; q < 4; ++q) {
+        g.relax[q] = (T)rl[q];
+        g.tol[q] = (double)(T)tl[q];
+    }
+    g.tol_mass = (double)(T)c.tol_mass;
+    for (int f = 0; f < 6; ++f) {
+        g.bc[f] = c.vel_bc_type[f];
+        g.closed[f] = c.vel_bc_type[f] != IFC_OUTLET;
+        for (int q = 0; q < 3; ++q) g.bcv[f][q] = (T)c.vel_bc_val[f][q];
+    }
+    g.inlet = nullptr;
+    g.criterion = c.criterion == IFC_CRIT_REFERENCE ? 0 : 1;
+    Derived<T> &d = P.d;
+    d.Dx = g.mu * g.Ax / g.dx;
+    d.Dy = g.mu * g.Ay / g.dy;
+    d.Dz = g.mu * g.Az / g.dz;
+    const double rho = (double)g.rho;
+    d.Kx = -0.5 * rho * (double)g.Ax * (double)g.Ax;
+    d.Ky = -0.5 * rho * (double)g.Ay * (double)g.Ay;
+    d.Kz = -0.5 * rho * (double)g.Az * (double)g.Az;
+    for (int q = 0; q < 3; ++q) d.ru[q] = (double)g.relax[q] * 0.5;
+    d.c83 = (T)8 / (T)3;
+    return P;
+}
+
+template <typename T>
+struct Engine : EngineBase {
+    ifc_config cfg;
+    Params<T> P;
+    Fields<T> f;
+    Ctl *ctl = nullptr;
+    double *partials = nullptr;
+    T *inlet_d = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int nsm = 148;
+    int max_grid = 148 * 8;
+    int dim = 2;
+    bool pin = false;
+    bool fused = false;               // 2D temporally blocked kernels
+    int spp_mom = 4, spp_p = 4;       // sweeps per pass of the fused kernels
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t body_graph = nullptr;
+    cudaGraphExec_t body_exec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void *> allocs;
+    Ctl ctl_h;
+    double last_ms = 0.0;
+    long long launches = 0;           // kernels enqueued (counted by the enq_* helpers)
+    long long launches_per_iter = 0;  // kernels in one captured outer iteration
+    long long last_launches = 0;
+
+    ~Engine() override
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (body_exec) cudaGraphExecDestroy(body_exec);
+        if (body_graph) cudaGraphDestroy(body_graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : allocs) cudaFree(p);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    int grid(long long work) const
+    {
+        long long b = (work + 255) / 256;
+        if (b < 1) b = 1;
+        if (b > max_grid) b = max_grid;
+        return (int)b;
+    }
+
+    template <typename U>
+    int alloc(U **p, size_t n)
+    {
+        void *q = nullptr;
+        IFC_CK(cudaMalloc(&q, n * sizeof(U) > 0 ? n * sizeof(U) : 16));
+        allocs.push_back(q);
+        *p = (U *)q;
+        return IFC_OK;
+    }
+
+    size_t nface(int which) const
+    {
+        const Geo<T> &g = P.g;
+        if (which == 0) return (size_t)(g.nx + 1) * g.ny * g.nz;
+        if (which == 1) return (size_t)g.nx * (g.ny + 1) * g.nz;
+        return (size_t)g.nx * g.ny * (g.nz + 1);
+    }
+
+    int init(const ifc_config &c)
+    {
+        cfg = c;
+        P = make_params<T>(c);
+        dim = P.g.dim;
+        const size_t N = (size_t)P.g.N, nc = (size_t)(2 * dim + 1);
+        int dev = 0;
+        IFC_CK(cudaGetDevice(&dev));
+        IFC_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        max_grid = nsm * 8;
+        if (c.stream) {
+            stream = (cudaStream_t)c.stream;
+        } else {
+            IFC_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own_stream = true;
+        }
+        IFC_CK(cudaEventCreate(&ev0));
+        IFC_CK(cudaEventCreate(&ev1));
+        std::memset(&f, 0, sizeof(f));
+        int rc;
+#define A_(ptr, n) if ((rc = alloc(&(ptr), (n))) != IFC_OK) return rc
+        A_(f.u, N); A_(f.v, N); A_(f.w, N); A_(f.p, N); A_(f.temp, N); A_(f.pc, N);
+        A_(f.uf, nface(0)); A_(f.vf, nface(1)); A_(f.wf, nface(2));
+        A_(f.ac, N); A_(f.mc, N * nc); A_(f.pcoef, N * nc);
+        A_(f.su, N); A_(f.sv, N); A_(f.sw, N); A_(f.sp, N); A_(f.tmp, 3 * N);
+        A_(partials, (size_t)max_grid * kMaxReduce + 4096 * 8);
+        A_(ctl, 1);
+#undef A_
+        if (c.inlet_profile) {
+            const size_t n = (size_t)P.g.ny * P.g.nz;
+            std::vector<T> h(n);
+            for (size_t q = 0; q < n; ++q) h[q] = (T)c.inlet_profile[q];
+            if ((rc = alloc(&inlet_d, n)) != IFC_OK) return rc;
+            IFC_CK(cudaMemcpy(inlet_d, h.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+            P.g.inlet = inlet_d;
+        }
+        bool closed = true;
+        for (int q = 0; q < 2 * dim; ++q) closed = closed && c.vel_bc_type[q] != IFC_OUTLET;
+        pin = c.pin_pressure == 1 || (c.pin_pressure < 0 && closed);
+        fused = (dim == 2) && fused2d_supported<T>(P.g);
+        if (c.sweeps_per_pass > 0) spp_mom = spp_p = c.sweeps_per_pass;
+        if ((rc = set_uniform(0.0, 0.0, 0.0, 0.0, 273.0)) != IFC_OK) return rc;
+        if ((rc = build_graph()) != IFC_OK) return rc;
+        return IFC_OK;
+    }
+
+    int set_uniform(double u, double v, double w, double p, double t) override
+    {
+        const long long N = P.g.N;
+        const int G = grid(N);
+        k_fill<T><<<G, 256, 0, stream>>>(f.u, N, (T)u);
+        k_fill<T><<<G, 256, 0, stream>>>(f.v, N, (T)v);
+        k_fill<T><<<G, 256, 0, stream>>>(f.w, N, (T)w);
+        k_fill<T><<<G, 256, 0, stream>>>(f.p, N, (T)p);
+        k_fill<T><<<G, 256, 0, stream>>>(f.temp, N, (T)t);
+        const size_t nc = (size_t)(2 * dim + 1);
+        IFC_CK(cudaMemsetAsync(f.pc, 0, N * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.uf, 0, nface(0) * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.vf, 0, nface(1) * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.wf, 0, nface(2) * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.ac, 0, N * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.mc, 0, N * nc * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.pcoef, 0, N * nc * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.su, 0, N * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.sv, 0, N * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.sw, 0, N * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(f.sp, 0, N * sizeof(T), stream));
+        IFC_CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), stream));
+        IFC_CK(cudaGetLastError());
+        IFC_CK(cudaStreamSynchronize(stream));
+        return IFC_OK;
+    }
+
+    T *field_ptr(int field) const
+    {
+        switch (field) {
+        case IFC_FIELD_U: return f.u;
+        case IFC_FIELD_V: return f.v;
+        case IFC_FIELD_W: return f.w;
+        case IFC_FIELD_P: return f.p;
+        case IFC_FIELD_T: return f.temp;
+        case IFC_FIELD_PCORR: return f.pc;
+        case IFC_FIELD_UF: return f.uf;
+        case IFC_FIELD_VF: return f.vf;
+        case IFC_FIELD_WF: return f.wf;
+        case IFC_FIELD_MOM_AC: return f.ac;
+        case IFC_FIELD_MOM_COEF: return f.mc;
+        case IFC_FIELD_PCORR_COEF: return f.pcoef;
+        case IFC_FIELD_SRC_U: return f.su;
+        case IFC_FIELD_SRC_V: return f.sv;
+        case IFC_FIELD_SRC_W: return f.sw;
+        case IFC_FIELD_SRC_P: return f.sp;
+        default: return nullptr;
+        }
+    }
+
+    size_t field_size(int field) const override
+    {
+        const size_t N = (size_t)P.g.N;
+        switch (field) {
+        case IFC_FIELD_UF: return nface(0) * sizeof(T);
+        case IFC_FIELD_VF: return nface(1) * sizeof(T);
+        case IFC_FIELD_WF: return nface(2) * sizeof(T);
+        case IFC_FIELD_MOM_COEF:
+        case IFC_FIELD_PCORR_COEF: return N * (size_t)(2 * dim + 1) * sizeof(T);
+        default: return field_ptr(field) ? N * sizeof(T) : 0;
+        }
+    }
+
+    void *device_ptr(int field) override { return field_ptr(field); }
+
+    int set_field(int field, const void *host, size_t bytes) override
+    {
+        T *d = field_ptr(field);
+        if (!d || !host || bytes != field_size(field)) {
+            err = "set_field: bad field id, pointer or size";
+            return IFC_BAD_ARGUMENT;
+        }
+        IFC_CK(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream));
+        IFC_CK(cudaStreamSynchronize(stream));
+        return IFC_OK;
+    }
+
+    int get_field(int field, void *host, size_t bytes) override
+    {
+        T *d = field_ptr(field);
+        if (!d || !host || bytes != field_size(field)) {
+            err = "get_field: bad field id, pointer or size";
+            return IFC_BAD_ARGUMENT;
+        }
+        IFC_CK(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, stream));
+        IFC_CK(cudaStreamSynchronize(stream));
+        return IFC_OK;
+    }
+
+    // ---- enqueue helpers (no synchronisation; usable under stream capture) ----
+    template <int DIM>
+    void enq_face_bc()
+    {
+        const long long nf = (long long)nface(0) + nface(1) + (DIM == 3 ? (long long)nface(2) : 0);
+        k_face_bc<T, DIM><<<grid(nf), 256, 0, stream>>>(P, f, ctl);
+        ++launches;
+    }
+
+    template <int DIM, int NC>
+    void enq_sweeps(const T *coef, T *const *phi, T *const *src, const int *eqs, const int *niter)
+    {
+        int nmax = 0;
+        for (int c = 0; c < NC; ++c) nmax = niter[c] > nmax ? niter[c] : nmax;
+        const bool jac = cfg.linear_solver == IFC_JACOBI;
+        const long long N = P.g.N;
+        const long long half = (long long)((P.g.nx + 1) / 2) * P.g.ny * P.g.nz;
+        for (int s = 0; s < nmax; ++s) {
+            SweepArgs<T, NC> A;
+            A.coef = coef;
+            for (int c = 0; c < NC; ++c) {
+                A.phi[c] = phi[c];
+                A.src[c] = src[c];
+                A.eq[c] = eqs[c];
+                A.active[c] = s < niter[c];
+                A.old[c] = jac ? f.tmp + (size_t)c * N : phi[c];
+            }
+            if (jac) {
+                A.color = -1;
+                k_copy_active<T, NC><<<grid(N), 256, 0, stream>>>(A, ctl, (int)N);
+                k_sweep<T, DIM, NC><<<grid(N), 256, 0, stream>>>(P, A, ctl, partials);
+                launches += 2;
+            } else {
+                A.color = 0;
+                k_sweep<T, DIM, NC><<<grid(half), 256, 0, stream>>>(P, A, ctl, partials);
+                A.color = 1;
+                k_sweep<T, DIM, NC><<<grid(half), 256, 0, stream>>>(P, A, ctl, partials);
+                launches += 2;
+            }
+        }
+    }
+
+    template <int DIM>
+    void enq_mom_assemble()
+    {
+        k_mom_assemble<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl);
+        ++launches;
+    }
+
+    template <int DIM>
+    void enq_mom_solve()
+    {
+        if (DIM == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+            enq_fused_mom();
+            return;
+        }
+        enq_mom_assemble<DIM>();
+        T *phi[3] = {f.u, f.v, f.w};
+        T *src[3] = {f.su, f.sv, f.sw};
+        const int eqs[3] = {EQ_U, EQ_V, EQ_W};
+        const int ni[3] = {cfg.n_iter_u, cfg.n_iter_v, cfg.n_iter_w};
+        enq_sweeps<DIM, DIM>(f.mc, phi, src, eqs, ni);
+    }
+
+    template <int DIM>
+    void enq_rhie_chow()
+    {
+        const long long nf = (long long)nface(0) + nface(1) + (DIM == 3 ? (long long)nface(2) : 0);
+        k_rhie_chow<T, DIM><<<grid(nf), 256, 0, stream>>>(P, f);
+        k_pcorr_src<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl, partials);
+        launches += 2;
+    }
+
+    template <int DIM>
+    void enq_pcorr_coef()
+    {
+        k_pcorr_coef<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl);
+        ++launches;
+    }
+
+    template <int DIM>
+    void enq_pcorr_solve()
+    {
+        if (DIM == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+            enq_fused_pcorr();
+        } else {
+            enq_pcorr_coef<DIM>();
+            cudaMemsetAsync(f.pc, 0, (size_t)P.g.N * sizeof(T), stream);
+            T *phi[1] = {f.pc};
+            T *src[1] = {f.sp};
+            const int eqs[1] = {EQ_P};
+            const int ni[1] = {cfg.n_iter_p};
+            enq_sweeps<DIM, 1>(f.pcoef, phi, src, eqs, ni);
+        }
+        if (pin) {
+            k_pc_sum<T><<<grid(P.g.N), 256, 0, stream>>>(f.pc, P.g.N, ctl, partials);
+            k_pc_shift<T><<<grid(P.g.N), 256, 0, stream>>>(f.pc, P.g.N, ctl);
+            launches += 2;
+        }
+    }
+
+    template <int DIM>
+    void enq_update(int use_cond)
+    {
+        k_update<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl, partials, cond, use_cond);
+        ++launches;
+    }
+
+    template <int DIM>
+    void enq_iteration(int use_cond)
+    {
+        enq_face_bc<DIM>();
+        enq_mom_solve<DIM>();
+        enq_rhie_chow<DIM>();
+        enq_pcorr_solve<DIM>();
+        enq_update<DIM>(use_cond);
+    }
+
+    void enq_iteration_any(int use_cond)
+    {
+        if (dim == 2) enq_iteration<2>(use_cond);
+        else enq_iteration<3>(use_cond);
+    }
+
+    // Fused 2D path (ifc_fused2d.cuh).
+    void enq_fused_mom();
+    void enq_fused_pcorr();
+
+    int build_graph()
+    {
+        // Preferred form: one graph whose WHILE node repeats the outer
+        // iteration until the update kernel clears the condition.
+        bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                  cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        if (ok) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+            if (ok) {
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                ok = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    const long long l0 = launches;
+                    enq_iteration_any(1);
+                    launches_per_iter = launches - l0;
+                    ok = cudaStreamEndCapture(stream, &body) == cudaSuccess;
+                }
+            }
+            ok = ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        }
+        if (!ok) {
+            cudaGetLastError();
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            exec = nullptr;
+            graph = nullptr;
+            cond = 0;
+            // Fallback: one captured outer iteration, relaunched from the host.
+            IFC_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            const long long l0 = launches;
+            enq_iteration_any(0);
+            launches_per_iter = launches - l0;
+            IFC_CK(cudaStreamEndCapture(stream, &body_graph));
+            IFC_CK(cudaGraphInstantiate(&body_exec, body_graph, 0));
+        }
+        IFC_CK(cudaGetLastError());
+        return IFC_OK;
+    }
+
+    int read_ctl()
+    {
+        IFC_CK(cudaMemcpyAsync(&ctl_h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+        IFC_CK(cudaStreamSynchronize(stream));
+        return IFC_OK;
+    }
+
+    void print_log()
+    {
+        for (int q = 0; q < ctl_h.log_n && q < kLogCap; ++q) {
+            const LogRec &L = ctl_h.log[q];
+            std::printf("iter: %d\n", L.it);
+            std::printf("pRelNorm : %.3E\n", L.rel[0]);
+            std::printf("uRelNorm : %.3E\n", L.rel[1]);
+            std::printf("vRelNorm : %.3E\n", L.rel[2]);
+            if (dim == 3) std::printf("wRelNorm : %.3E\n", L.rel[3]);
+            std::printf("ufRelNorm: %.3E\n", L.rel[4]);
+            std::printf("vfRelNorm: %.3E\n", L.rel[5]);
+            if (dim == 3) std::printf("wfRelNorm: %.3E\n", L.rel[6]);
+            std::printf("massNorm : %.3E\n", L.mass);
+            std::printf("------------------------------------------------------------\n");
+        }
+        std::fflush(stdout);
+    }
+
+    void fill_stats(ifc_stats *st)
+    {
+        if (!st) return;
+        std::memset(st, 0, sizeof(*st));
+        st->outer_iterations = ctl_h.it;
+        st->converged = ctl_h.converged;
+        for (int q = 0; q < 4; ++q) st->sweeps[q] = ctl_h.sweeps[q];
+        st->cell_updates = ctl_h.cell_updates;
+        const double *n = ctl_h.norm, *r = ctl_h.rel;
+        st->norm_p = n[0]; st->norm_u = n[1]; st->norm_v = n[2]; st->norm_w = n[3];
+        st->norm_uf = n[4]; st->norm_vf = n[5]; st->norm_wf = n[6]; st->norm_mass = n[7];
+        st->rel_p = r[0]; st->rel_u = r[1]; st->rel_v = r[2]; st->rel_w = r[3];
+        st->rel_uf = r[4]; st->rel_vf = r[5]; st->rel_wf = r[6];
+        st->device_ms = last_ms;
+        st->kernel_launches = last_launches;
+    }
+
+    int run(int n_outer, int act, ifc_stats *st) override
+    {
+        if (n_outer < 0) {
+            err = "negative iteration count";
+            return IFC_BAD_ARGUMENT;
+        }
+        int rc;
+        if (n_outer == 0) {
+            if ((rc = read_ctl()) != IFC_OK) return rc;
+            last_ms = 0.0;
+            fill_stats(st);
+            if (st) st->status = IFC_OK;
+            return IFC_OK;
+        }
+        k_begin<<<1, 1, 0, stream>>>(ctl, n_outer, act, cfg.log_level);
+        IFC_CK(cudaEventRecord(ev0, stream));
+        if (exec) {
+            IFC_CK(cudaGraphLaunch(exec, stream));
+        } else {
+            for (int q = 0; q < n_outer; ++q) {
+                IFC_CK(cudaGraphLaunch(body_exec, stream));
+                if ((rc = read_ctl()) != IFC_OK) return rc;
+                if (ctl_h.status || (act && ctl_h.converged)) break;
+            }
+        }
+        IFC_CK(cudaEventRecord(ev1, stream));
+        IFC_CK(cudaStreamSynchronize(stream));
+        IFC_CK(cudaGetLastError());
+        float ms = 0.f;
+        IFC_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        if ((rc = read_ctl()) != IFC_OK) return rc;
+        if (cfg.log_level > 0) print_log();
+        fill_stats(st);
+        int status = IFC_OK;
+        last_launches = (long long)(ctl_h.it - ctl_h.it_begin) * launches_per_iter;
+        if (ctl_h.status == 2) status = IFC_DIVERGED;
+        else if (act && !ctl_h.converged) status = IFC_NOT_CONVERGED;
+        if (st) st->status = status;
+        return status;
+    }
+
+    int run_stage(int stage) override
+    {
+        if (stage < 0 || stage >= IFC_STAGE_COUNT) {
+            err = "unknown stage";
+            return IFC_BAD_ARGUMENT;
+        }
+        if (dim == 2) run_stage_t<2>(stage);
+        else run_stage_t<3>(stage);
+        IFC_CK(cudaGetLastError());
+        IFC_CK(cudaStreamSynchronize(stream));
+        return read_ctl();
+    }
+
+    template <int DIM>
+    void run_stage_t(int stage)
+    {
+        switch (stage) {
+        case IFC_STAGE_FACE_BC: enq_face_bc<DIM>(); break;
+        case IFC_STAGE_MOM_ASSEMBLE: enq_mom_assemble<DIM>(); break;
+        case IFC_STAGE_MOM_SOLVE: enq_mom_solve<DIM>(); break;
+        case IFC_STAGE_RHIE_CHOW: enq_rhie_chow<DIM>(); break;
+        case IFC_STAGE_PCORR_COEF: enq_pcorr_coef<DIM>(); break;
+        case IFC_STAGE_PCORR_SOLVE: enq_pcorr_solve<DIM>(); break;
+        case IFC_STAGE_UPDATE:
+            k_begin<<<1, 1, 0, stream>>>(ctl, 1, 0, 0);
+            enq_update<DIM>(0);
+            break;
+        }
+    }
+
+    int time_stage(int stage, int reps, double *ms, int *nl) override
+    {
+        if (stage < 0 || stage >= IFC_STAGE_COUNT || reps < 1 || !ms) {
+            err = "time_stage: bad stage or count";
+            return IFC_BAD_ARGUMENT;
+        }
+        IFC_CK(cudaStreamSynchronize(stream));
+        const long long l0 = launches;
+        IFC_CK(cudaEventRecord(ev0, stream));
+        for (int r = 0; r < reps; ++r) {
+            if (dim == 2) run_stage_t<2>(stage);
+            else run_stage_t<3>(stage);
+        }
+        IFC_CK(cudaEventRecord(ev1, stream));
+        IFC_CK(cudaStreamSynchronize(stream));
+        IFC_CK(cudaGetLastError());
+        float t = 0.f;
+        IFC_CK(cudaEventElapsedTime(&t, ev0, ev1));
+        *ms = (double)t / reps;
+        if (nl) *nl = (int)((launches - l0) / reps);
+        return IFC_OK;
+    }
+
+    int sweep(int eq, int n, double *sq) override
+    {
+        if (eq < 0 || eq > 3 || (eq == 2 && dim == 2) || n < 0) {
+            err = "sweep: bad equation or count";
+            return IFC_BAD_ARGUMENT;
+        }
+        T *phi[1] = {eq == 0 ? f.u : eq == 1 ? f.v : eq == 2 ? f.w : f.pc};
+        T *src[1] = {eq == 0 ? f.su : eq == 1 ? f.sv : eq == 2 ? f.sw : f.sp};
+        const int eqs[1] = {eq};
+        const int one[1] = {1};
+        for (int s = 0; s < n; ++s) {
+            k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << eq);
+            if (dim == 2) enq_sweeps<2, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
+            else enq_sweeps<3, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
+            IFC_CK(cudaGetLastError());
+            int rc = read_ctl();
+            if (rc != IFC_OK) return rc;
+            if (sq) sq[s] = ctl_h.last_sweep_sq[eq];
+        }
+        return IFC_OK;
+    }
+
+    int stats(ifc_stats *st) override
+    {
+        int rc = read_ctl();
+        if (rc != IFC_OK) return rc;
+        fill_stats(st);
+        if (st) st->status = IFC_OK;
+        return IFC_OK;
+    }
+};
+
+}  // namespace ifc

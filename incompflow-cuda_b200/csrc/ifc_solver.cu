@@ -1,0 +1,250 @@
+// ifc_solver.cu -- C ABI of the solver (include/ifc.h).  Every entry point
+// validates its arguments, catches C++ exceptions and returns a status code;
+// the reference has no error reporting at all (its defect D11).
+#include <cstring>
+#include <new>
+
+#include "ifc.h"
+#include "ifc_engine.cuh"
+
+using ifc::EngineBase;
+
+struct ifc_solver {
+    ifc_config cfg;
+    EngineBase *eng;
+    std::string err;
+};
+
+#include "ifc_fused2d_impl.cuh"
+
+extern "C" {
+
+int ifc_abi_version(void) { return IFC_ABI_VERSION; }
+
+const char *ifc_status_string(int s)
+{
+    switch (s) {
+    case IFC_OK: return "ok";
+    case IFC_NOT_CONVERGED: return "not converged";
+    case IFC_DIVERGED: return "diverged";
+    case IFC_TIMEOUT: return "timeout";
+    case IFC_CUDA_ERROR: return "CUDA error";
+    case IFC_BAD_CONFIG: return "bad configuration";
+    case IFC_BAD_ARGUMENT: return "bad argument";
+    case IFC_IO_ERROR: return "I/O error";
+    case IFC_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+    }
+}
+
+// include/config.h:6-81 as shipped by the reference.
+int ifc_config_default(ifc_config *c)
+{
+    if (!c) return IFC_BAD_ARGUMENT;
+    std::memset(c, 0, sizeof(*c));
+    c->dim = 2;
+    c->nx = 1024;
+    c->ny = 256;
+    c->nz = 1;
+    c->xmin = -2; c->xmax = 2; c->ymin = -0.5; c->ymax = 0.5; c->zmin = 0.0; c->zmax = 1.0;
+    c->thermal_conductivity = 1;
+    c->specific_heat_capacity = 1;
+    c->density = 50;
+    c->dynamic_viscosity = 1;
+    const int vt[6] = {IFC_OUTLET, IFC_INLET, IFC_WALL, IFC_WALL, IFC_WALL, IFC_WALL};
+    for (int f = 0; f < 6; ++f) c->vel_bc_type[f] = vt[f];
+    c->vel_bc_val[IFC_WEST][0] = 1;
+    const int tt[6] = {1, 1, 0, 0, 1, 1};
+    const double tv[6] = {0.0, 0.0, 293.0, 373.0, 0.0, 0.0};
+    for (int f = 0; f < 6; ++f) { c->temp_bc_type[f] = tt[f]; c->temp_bc_val[f] = tv[f]; }
+    c->num_outer_iter = 20000;
+    c->n_iter_u = 10; c->n_iter_v = 10; c->n_iter_w = 10; c->n_iter_p = 20;
+    c->relax_u = 0.75; c->relax_v = 0.75; c->relax_w = 0.75; c->relax_p = 0.25;
+    c->tol_u = 1e-5; c->tol_v = 1e-5; c->tol_w = 1e-5; c->tol_p = 1e-3; c->tol_mass = 1e-9;
+    c->precision = IFC_FP32;
+    c->linear_solver = IFC_GAUSS_SEIDEL;
+    c->criterion = IFC_CRIT_PER_FIELD;
+    c->pin_pressure = -1;
+    c->sweeps_per_pass = 0;
+    c->log_level = 0;
+    c->inlet_profile = nullptr;
+    c->stream = nullptr;
+    return IFC_OK;
+}
+
+int ifc_config_check(const ifc_config *c)
+{
+    if (!c) return IFC_BAD_ARGUMENT;
+    if (c->dim != 2 && c->dim != 3) return IFC_BAD_CONFIG;
+    const int nz = c->dim == 2 ? 1 : c->nz;
+    if (c->nx < 3 || c->ny < 3 || (c->dim == 3 && nz < 3)) return IFC_BAD_CONFIG;
+    if ((double)c->nx * c->ny * nz > (double)(1 << 28)) return IFC_BAD_CONFIG;
+    if (!(c->xmax > c->xmin) || !(c->ymax > c->ymin) || !(c->zmax > c->zmin)) return IFC_BAD_CONFIG;
+    for (int f = 0; f < 6; ++f)
+        if (c->vel_bc_type[f] < IFC_WALL || c->vel_bc_type[f] > IFC_OUTLET) return IFC_BAD_CONFIG;
+    if (c->num_outer_iter < 0 || c->n_iter_u < 0 || c->n_iter_v < 0 || c->n_iter_w < 0 || c->n_iter_p < 0)
+        return IFC_BAD_CONFIG;
+    if (c->n_iter_u > 100000 || c->n_iter_v > 100000 || c->n_iter_w > 100000 || c->n_iter_p > 100000)
+        return IFC_BAD_CONFIG;
+    if (c->precision != IFC_FP32 && c->precision != IFC_FP64) return IFC_BAD_CONFIG;
+    if (c->linear_solver != IFC_GAUSS_SEIDEL && c->linear_solver != IFC_JACOBI) return IFC_BAD_CONFIG;
+    if (c->criterion != IFC_CRIT_REFERENCE && c->criterion != IFC_CRIT_PER_FIELD) return IFC_BAD_CONFIG;
+    if (c->pin_pressure < -1 || c->pin_pressure > 1) return IFC_BAD_CONFIG;
+    if (c->sweeps_per_pass < 0 || c->sweeps_per_pass > 16) return IFC_BAD_CONFIG;
+    return IFC_OK;
+}
+
+int ifc_create(const ifc_config *cfg, ifc_solver **out)
+{
+    if (!cfg || !out) return IFC_BAD_ARGUMENT;
+    *out = nullptr;
+    int rc = ifc_config_check(cfg);
+    if (rc != IFC_OK) return rc;
+    ifc_solver *h = new (std::nothrow) ifc_solver;
+    if (!h) return IFC_CUDA_ERROR;
+    h->cfg = *cfg;
+    if (h->cfg.dim == 2) h->cfg.nz = 1;
+    h->eng = nullptr;
+    try {
+        if (cfg->precision == IFC_FP64) {
+            auto *e = new ifc::Engine<double>();
+            h->eng = e;
+            rc = e->init(h->cfg);
+        } else {
+            auto *e = new ifc::Engine<float>();
+            h->eng = e;
+            rc = e->init(h->cfg);
+        }
+    } catch (const std::exception &ex) {
+        h->err = ex.what();
+        rc = IFC_CUDA_ERROR;
+    }
+    if (rc != IFC_OK) {
+        delete h->eng;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return IFC_OK;
+}
+
+int ifc_destroy(ifc_solver *h)
+{
+    if (!h) return IFC_OK;
+    delete h->eng;
+    delete h;
+    return IFC_OK;
+}
+
+#define IFC_GUARD(h)                             \
+    if (!(h) || !(h)->eng) return IFC_BAD_ARGUMENT; \
+    try {
+#define IFC_END(h)                               \
+    }                                            \
+    catch (const std::exception &ex) {           \
+        (h)->eng->err = ex.what();               \
+        return IFC_CUDA_ERROR;                   \
+    }
+
+int ifc_set_uniform(ifc_solver *h, double u, double v, double w, double p, double temp)
+{
+    IFC_GUARD(h)
+    return h->eng->set_uniform(u, v, w, p, temp);
+    IFC_END(h)
+}
+
+int ifc_set_field(ifc_solver *h, int field, const void *host, size_t bytes)
+{
+    IFC_GUARD(h)
+    return h->eng->set_field(field, host, bytes);
+    IFC_END(h)
+}
+
+int ifc_get_field(ifc_solver *h, int field, void *host, size_t bytes)
+{
+    IFC_GUARD(h)
+    return h->eng->get_field(field, host, bytes);
+    IFC_END(h)
+}
+
+size_t ifc_field_size(const ifc_solver *h, int field)
+{
+    if (!h || !h->eng) return 0;
+    return h->eng->field_size(field);
+}
+
+int ifc_device_ptr(ifc_solver *h, int field, void **dptr)
+{
+    if (!dptr) return IFC_BAD_ARGUMENT;
+    IFC_GUARD(h)
+    *dptr = h->eng->device_ptr(field);
+    return *dptr ? IFC_OK : IFC_BAD_ARGUMENT;
+    IFC_END(h)
+}
+
+int ifc_solve(ifc_solver *h, ifc_stats *stats)
+{
+    IFC_GUARD(h)
+    return h->eng->run(h->cfg.num_outer_iter, 1, stats);
+    IFC_END(h)
+}
+
+int ifc_iterate(ifc_solver *h, int n_outer, ifc_stats *stats)
+{
+    IFC_GUARD(h)
+    return h->eng->run(n_outer, 0, stats);
+    IFC_END(h)
+}
+
+int ifc_run_stage(ifc_solver *h, int stage)
+{
+    IFC_GUARD(h)
+    return h->eng->run_stage(stage);
+    IFC_END(h)
+}
+
+int ifc_sweep(ifc_solver *h, int eq, int n, double *sq_norms)
+{
+    IFC_GUARD(h)
+    return h->eng->sweep(eq, n, sq_norms);
+    IFC_END(h)
+}
+
+int ifc_time_stage(ifc_solver *h, int stage, int reps, double *ms, int *launches)
+{
+    IFC_GUARD(h)
+    return h->eng->time_stage(stage, reps, ms, launches);
+    IFC_END(h)
+}
+
+int ifc_get_stats(ifc_solver *h, ifc_stats *stats)
+{
+    IFC_GUARD(h)
+    return h->eng->stats(stats);
+    IFC_END(h)
+}
+
+int ifc_write_vtk(ifc_solver *h, const char *path)
+{
+    if (!path) return IFC_BAD_ARGUMENT;
+    IFC_GUARD(h)
+    const size_t bytes = h->eng->field_size(IFC_FIELD_U);
+    std::vector<char> u(bytes), v(bytes), w(bytes), p(bytes), t(bytes);
+    int rc;
+    if ((rc = h->eng->get_field(IFC_FIELD_U, u.data(), bytes)) != IFC_OK) return rc;
+    if ((rc = h->eng->get_field(IFC_FIELD_V, v.data(), bytes)) != IFC_OK) return rc;
+    if ((rc = h->eng->get_field(IFC_FIELD_W, w.data(), bytes)) != IFC_OK) return rc;
+    if ((rc = h->eng->get_field(IFC_FIELD_P, p.data(), bytes)) != IFC_OK) return rc;
+    if ((rc = h->eng->get_field(IFC_FIELD_T, t.data(), bytes)) != IFC_OK) return rc;
+    return ifc_write_vtk_host(&h->cfg, u.data(), v.data(), w.data(), p.data(), t.data(), path);
+    IFC_END(h)
+}
+
+const char *ifc_last_error(const ifc_solver *h)
+{
+    if (!h) return "null handle";
+    if (h->eng && !h->eng->err.empty()) return h->eng->err.c_str();
+    return h->err.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+"""ctypes binding of libifc.so (the C ABI in include/ifc.h).
+
+This is the Python face of the drop-in solver: tests and bench.py drive the
+CUDA library through it.  It never falls back to anything: if the built
+library is missing, ``load()`` raises.
+
+Configurations are dicts keyed by the reference's config.h names
+(include/config.h:6-81): ``dim, nx, ny, nz, xmin..zmax, density,
+dynamicViscosity, velBC_type, velBC_val, numOuterIter, nIter_u/v/w/p,
+relax_u/v/w/p, tol_u/v/w/p, tol_mass`` plus the additions ``precision``
+("f"/"d"), ``linear_solver``, ``criterion``, ``pin_pressure``,
+``sweeps_per_pass``, ``log_level`` and ``inlet_profile``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libifc.so")
+
+OK, NOT_CONVERGED, DIVERGED, TIMEOUT, CUDA_ERROR, BAD_CONFIG, BAD_ARGUMENT, IO_ERROR, UNSUPPORTED = range(9)
+EAST, WEST, NORTH, SOUTH, TOP, BOTTOM = range(6)
+WALL, INLET, OUTLET = range(3)
+GAUSS_SEIDEL, JACOBI = 0, 1
+CRIT_REFERENCE, CRIT_PER_FIELD = 0, 1
+FIELDS = ["u", "v", "w", "p", "T", "pc", "uf", "vf", "wf", "ac", "mcoef", "pcoef",
+          "src_u", "src_v", "src_w", "src_p"]
+STAGES = ["face_bc", "mom_assemble", "mom_solve", "rhie_chow", "pcorr_coef", "pcorr_solve", "update"]
+
+
+class IfcConfig(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+        ("zmin", C.c_double), ("zmax", C.c_double),
+        ("thermal_conductivity", C.c_double), ("specific_heat_capacity", C.c_double),
+        ("density", C.c_double), ("dynamic_viscosity", C.c_double),
+        ("vel_bc_type", C.c_int * 6), ("vel_bc_val", (C.c_double * 3) * 6),
+        ("temp_bc_type", C.c_int * 6), ("temp_bc_val", C.c_double * 6),
+        ("num_outer_iter", C.c_int),
+        ("n_iter_u", C.c_int), ("n_iter_v", C.c_int), ("n_iter_w", C.c_int), ("n_iter_p", C.c_int),
+        ("relax_u", C.c_double), ("relax_v", C.c_double), ("relax_w", C.c_double), ("relax_p", C.c_double),
+        ("tol_u", C.c_double), ("tol_v", C.c_double), ("tol_w", C.c_double), ("tol_p", C.c_double),
+        ("tol_mass", C.c_double),
+        ("precision", C.c_int), ("linear_solver", C.c_int), ("criterion", C.c_int),
+        ("pin_pressure", C.c_int), ("sweeps_per_pass", C.c_int), ("log_level", C.c_int),
+        ("inlet_profile", C.POINTER(C.c_double)), ("stream", C.c_void_p),
+    ]
+
+
+class IfcStats(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("outer_iterations", C.c_int), ("converged", C.c_int),
+        ("sweeps", C.c_int * 4), ("cell_updates", C.c_longlong),
+    ] + [(n, C.c_double) for n in (
+        "norm_p", "norm_u", "norm_v", "norm_w", "norm_uf", "norm_vf", "norm_wf", "norm_mass",
+        "rel_p", "rel_u", "rel_v", "rel_w", "rel_uf", "rel_vf", "rel_wf", "device_ms")] + [
+        ("kernel_launches", C.c_longlong)]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_ if n != "sweeps"}
+        d["sweeps"] = list(self.sweeps)
+        return d
+
+
+EXPORTS = {
+    "ifc_abi_version": (C.c_int, []),
+    "ifc_status_string": (C.c_char_p, [C.c_int]),
+    "ifc_config_default": (C.c_int, [C.POINTER(IfcConfig)]),
+    "ifc_config_check": (C.c_int, [C.POINTER(IfcConfig)]),
+    "ifc_create": (C.c_int, [C.POINTER(IfcConfig), C.POINTER(C.c_void_p)]),
+    "ifc_destroy": (C.c_int, [C.c_void_p]),
+    "ifc_set_uniform": (C.c_int, [C.c_void_p] + [C.c_double] * 5),
+    "ifc_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    "ifc_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    "ifc_field_size": (C.c_size_t, [C.c_void_p, C.c_int]),
+    "ifc_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "ifc_solve": (C.c_int, [C.c_void_p, C.POINTER(IfcStats)]),
+    "ifc_iterate": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(IfcStats)]),
+    "ifc_write_vtk": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ifc_write_vtk_host": (C.c_int, [C.POINTER(IfcConfig)] + [C.c_void_p] * 5 + [C.c_char_p]),
+    "ifc_run_stage": (C.c_int, [C.c_void_p, C.c_int]),
+    "ifc_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "ifc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(IfcStats)]),
+    "ifc_time_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "ifc_last_error": (C.c_char_p, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libifc.so; raises OSError when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"{path} is missing: build it with `make -C incompflow-cuda_b200` "
+                          "or __graft_entry__.build()")
+        lib = C.CDLL(path)
+        for name, (res, args) in EXPORTS.items():
+            fn = getattr(lib, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class IfcError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        s = load().ifc_status_string(status).decode()
+        super().__init__(f"{s} ({status}){': ' + msg if msg else ''}")
+
+
+# ---------------------------------------------------------------- configs
+
+def default_config() -> dict:
+    """The reference's shipped include/config.h."""
+    return dict(
+        dim=2, nx=1024, ny=256, nz=1, xmin=-2.0, xmax=2.0, ymin=-0.5, ymax=0.5, zmin=0.0, zmax=1.0,
+        thermalConductivity=1.0, specificHeatCapacity=1.0, density=50.0, dynamicViscosity=1.0,
+        velBC_type=[OUTLET, INLET, WALL, WALL, WALL, WALL],
+        velBC_val=[[0, 0, 0], [1, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]],
+        TempBC_type=[1, 1, 0, 0, 1, 1], TempBC_val=[0.0, 0.0, 293.0, 373.0, 0.0, 0.0],
+        numOuterIter=20000, nIter_u=10, nIter_v=10, nIter_w=10, nIter_p=20,
+        relax_u=0.75, relax_v=0.75, relax_w=0.75, relax_p=0.25,
+        tol_u=1e-5, tol_v=1e-5, tol_w=1e-5, tol_p=1e-3, tol_mass=1e-9,
+    )
+
+
+def cavity2d(n: int = 64, re: float = 100.0, **kw) -> dict:
+    """Lid-driven cavity on the unit square: lid u=1 on the north wall,
+    rho=1, mu=1/Re, SIMPLE alpha_u=0.7 alpha_p=0.3, GS 5/5/50, residual 1e-5."""
+    c = default_config()
+    c.update(dim=2, nx=n, ny=n, nz=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
+             density=1.0, dynamicViscosity=1.0 / re, velBC_type=[WALL] * 6,
+             velBC_val=[[0, 0, 0], [0, 0, 0], [1, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]],
+             numOuterIter=20000, nIter_u=5, nIter_v=5, nIter_w=5, nIter_p=50,
+             relax_u=0.7, relax_v=0.7, relax_w=0.7, relax_p=0.3,
+             tol_u=1e-5, tol_v=1e-5, tol_w=1e-5, tol_p=1e-5, tol_mass=0.0)
+    c.update(kw)
+    return c
+
+
+def channel2d(nx: int = 512, ny: int = 128, u_in: float = 0.001, **kw) -> dict:
+    """The reference README's default case: water in a 0.125 x 0.025 m channel,
+    west inlet, east outlet, no-slip north/south; alpha 0.75/0.25, GS 10/10/20."""
+    c = default_config()
+    c.update(dim=2, nx=nx, ny=ny, nz=1, xmin=-0.0625, xmax=0.0625, ymin=-0.0125, ymax=0.0125,
+             zmin=0.0, zmax=1.0, density=998.2, dynamicViscosity=1.002e-3,
+             velBC_type=[OUTLET, INLET, WALL, WALL, WALL, WALL],
+             velBC_val=[[0, 0, 0], [u_in, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]],
+             numOuterIter=100000, nIter_u=10, nIter_v=10, nIter_w=10, nIter_p=20,
+             relax_u=0.75, relax_v=0.75, relax_w=0.75, relax_p=0.25,
+             tol_u=1e-5, tol_v=1e-5, tol_w=1e-5, tol_p=1e-5, tol_mass=0.0)
+    c.update(kw)
+    return c
+
+
+def cavity3d(n: int = 128, re: float = 400.0, **kw) -> dict:
+    """Lid-driven cube: lid u=1 on the top (z-max) wall, rho=1, mu=1/Re;
+    solver settings as the 2D cavity."""
+    c = cavity2d(n, re)
+    c.update(dim=3, nz=n, velBC_type=[WALL] * 6,
+             velBC_val=[[0, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0], [1, 0, 0], [0, 0, 0]])
+    c.update(kw)
+    return c
+
+
+def make_struct(cfg: dict) -> tuple[IfcConfig, object]:
+    c = IfcConfig()
+    load().ifc_config_default(C.byref(c))
+    c.dim = int(cfg["dim"])
+    c.nx, c.ny = int(cfg["nx"]), int(cfg["ny"])
+    c.nz = int(cfg.get("nz", 1)) if c.dim == 3 else 1
+    for k in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax"):
+        setattr(c, k, float(cfg[k]))
+    c.thermal_conductivity = float(cfg.get("thermalConductivity", 1.0))
+    c.specific_heat_capacity = float(cfg.get("specificHeatCapacity", 1.0))
+    c.density = float(cfg["density"])
+    c.dynamic_viscosity = float(cfg["dynamicViscosity"])
+    for f in range(6):
+        c.vel_bc_type[f] = int(cfg["velBC_type"][f])
+        for q in range(3):
+            c.vel_bc_val[f][q] = float(cfg["velBC_val"][f][q])
+    c.num_outer_iter = int(cfg["numOuterIter"])
+    for n in "uvwp":
+        setattr(c, f"n_iter_{n}", int(cfg[f"nIter_{n}"]))
+        setattr(c, f"relax_{n}", float(cfg[f"relax_{n}"]))
+        setattr(c, f"tol_{n}", float(cfg[f"tol_{n}"]))
+    c.tol_mass = float(cfg["tol_mass"])
+    c.precision = 1 if cfg.get("precision", "f") in ("d", 1, "fp64", "double") else 0
+    c.linear_solver = int(cfg.get("linear_solver", GAUSS_SEIDEL))
+    c.criterion = int(cfg.get("criterion", CRIT_PER_FIELD))
+    c.pin_pressure = int(cfg.get("pin_pressure", -1))
+    c.sweeps_per_pass = int(cfg.get("sweeps_per_pass", 0))
+    c.log_level = int(cfg.get("log_level", 0))
+    if cfg.get("stream"):
+        c.stream = C.c_void_p(int(cfg["stream"]))
+    keep = None
+    if cfg.get("inlet_profile") is not None:
+        keep = np.ascontiguousarray(cfg["inlet_profile"], dtype=np.float64)
+        c.inlet_profile = keep.ctypes.data_as(C.POINTER(C.c_double))
+    return c, keep
+
+
+class Solver:
+    """One solver handle (Solver::Solver ... Solver::~Solver of the reference)."""
+
+    def __init__(self, cfg: dict, u=0.0, v=0.0, w=0.0, p=0.0, temp=273.0):
+        lib = load()
+        self.cfg = dict(cfg)
+        self._struct, self._keep = make_struct(cfg)
+        h = C.c_void_p()
+        rc = lib.ifc_create(C.byref(self._struct), C.byref(h))
+        if rc != OK:
+            raise IfcError(rc, "ifc_create")
+        self._h = h
+        self.dtype = np.float64 if self._struct.precision == 1 else np.float32
+        self.dim, self.nx, self.ny, self.nz = self._struct.dim, self._struct.nx, self._struct.ny, self._struct.nz
+        self.N = self.nx * self.ny * self.nz
+        if (u, v, w, p, temp) != (0.0, 0.0, 0.0, 0.0, 273.0):
+            self.set_uniform(u, v, w, p, temp)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().ifc_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what, allow=(OK,)):
+        if rc not in allow:
+            msg = load().ifc_last_error(self._h)
+            raise IfcError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    def set_uniform(self, u=0.0, v=0.0, w=0.0, p=0.0, temp=273.0):
+        self._check(load().ifc_set_uniform(self._h, u, v, w, p, temp), "set_uniform")
+
+    def field_size(self, name: str) -> int:
+        return load().ifc_field_size(self._h, FIELDS.index(name))
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.field_size(name)
+        out = np.empty(n // np.dtype(self.dtype).itemsize, dtype=self.dtype)
+        self._check(load().ifc_get_field(self._h, FIELDS.index(name), out.ctypes.data, n), f"get {name}")
+        return out
+
+    def set(self, name: str, arr):
+        a = np.ascontiguousarray(arr, dtype=self.dtype).ravel()
+        self._check(load().ifc_set_field(self._h, FIELDS.index(name), a.ctypes.data, a.nbytes), f"set {name}")
+
+    def device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        self._check(load().ifc_device_ptr(self._h, FIELDS.index(name), C.byref(p)), "device_ptr")
+        return p.value
+
+    def solve(self) -> dict:
+        st = IfcStats()
+        self._check(load().ifc_solve(self._h, C.byref(st)), "solve", allow=(OK, NOT_CONVERGED))
+        return st.as_dict()
+
+    def iterate(self, n: int) -> dict:
+        st = IfcStats()
+        self._check(load().ifc_iterate(self._h, int(n), C.byref(st)), "iterate")
+        return st.as_dict()
+
+    def stage(self, name: str):
+        self._check(load().ifc_run_stage(self._h, STAGES.index(name)), f"stage {name}")
+
+    def sweep(self, eq: int, n: int = 1) -> np.ndarray:
+        sq = (C.c_double * max(n, 1))()
+        self._check(load().ifc_sweep(self._h, eq, n, sq), "sweep")
+        return np.array(sq[:n])
+
+    def time_stage(self, name: str, reps: int = 10) -> tuple[float, int]:
+        """Average device ms of one launch sequence of a stage, and its kernel count."""
+        ms, nl = C.c_double(), C.c_int()
+        self._check(load().ifc_time_stage(self._h, STAGES.index(name), reps, C.byref(ms), C.byref(nl)),
+                    "time_stage")
+        return ms.value, nl.value
+
+    def stats(self) -> dict:
+        st = IfcStats()
+        self._check(load().ifc_get_stats(self._h, C.byref(st)), "stats")
+        return st.as_dict()
+
+    def write_vtk(self, path: str):
+        self._check(load().ifc_write_vtk(self._h, path.encode()), "write_vtk")
+
+
+def write_vtk_host(cfg: dict, u, v, w, p, temp, path: str):
+    """The VTK writer on host arrays (no GPU)."""
+    s, keep = make_struct(cfg)
+    dt = np.float64 if s.precision == 1 else np.float32
+    arrs = [np.ascontiguousarray(a, dtype=dt).ravel() for a in (u, v, w, p, temp)]
+    rc = load().ifc_write_vtk_host(C.byref(s), *[a.ctypes.data for a in arrs], path.encode())
+    if rc != OK:
+        raise IfcError(rc, "write_vtk_host")

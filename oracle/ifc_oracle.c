@@ -1,0 +1,22 @@
+/*
+ * ifc_oracle.c -- instantiates the CPU oracle (TEST INFRASTRUCTURE ONLY) in
+ * float and double.  Build with -ffp-contract=off so that every operation is
+ * rounded as written; see ifc_oracle.h for scope and deviations.
+ */
+#include "ifc_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define T float
+#define S f
+#include "ifc_oracle_impl.h"
+#undef T
+#undef S
+
+#define T double
+#define S d
+#include "ifc_oracle_impl.h"
+#undef T
+#undef S

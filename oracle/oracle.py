@@ -1,0 +1,200 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is a serial C restatement of the reference solver's kernels
+(WanZijun271/IncompFlow-CUDA include/kernels.cuh:10-1005, driven in the order of
+src/Solver.cu:153-299); see ifc_oracle.h.  Only tests/, the smoke check and the
+cpu_baseline leg of bench.py import this module.  The product never does.
+
+Configurations are plain dicts whose keys follow the reference's config.h names
+(``nx``, ``density``, ``dynamicViscosity``, ``velBC_type``, ``nIter_u`` ...); the
+same dicts drive the CUDA library's binding.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libifc_oracle.so")
+
+GS_LEX, GS_REDBLACK, JACOBI = 0, 1, 2
+CRIT_REFERENCE, CRIT_PER_FIELD = 0, 1
+EQ_U, EQ_V, EQ_W, EQ_P = 0, 1, 2, 3
+FIELDS = ["u", "v", "w", "p", "pc", "uf", "vf", "wf", "mcoef", "pcoef", "src_u", "src_v", "src_w", "src_p"]
+
+
+class OrcConfig(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+        ("zmin", C.c_double), ("zmax", C.c_double),
+        ("density", C.c_double), ("viscosity", C.c_double),
+        ("bc_type", C.c_int * 6), ("bc_val", (C.c_double * 3) * 6),
+        ("num_outer_iter", C.c_int), ("n_iter", C.c_int * 4),
+        ("relax", C.c_double * 4), ("tol", C.c_double * 4), ("tol_mass", C.c_double),
+        ("sweep_mode", C.c_int), ("check_every", C.c_int), ("criterion", C.c_int),
+        ("pin_pressure", C.c_int), ("inlet_profile", C.POINTER(C.c_double)),
+    ]
+
+
+class OrcNorms(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("p", "u", "v", "w", "uf", "vf", "wf", "mass",
+                                           "rel_p", "rel_u", "rel_v", "rel_w", "rel_uf", "rel_vf", "rel_wf")] + [
+        ("sweeps", C.c_int * 4), ("converged", C.c_int)]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_ if n != "sweeps"}
+        d["sweeps"] = list(self.sweeps)
+        return d
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with gcc (make -C oracle); returns the library path."""
+    if force or not os.path.exists(LIB_PATH) or _stale():
+        subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    return LIB_PATH
+
+
+def _stale() -> bool:
+    t = os.path.getmtime(LIB_PATH)
+    return any(os.path.getmtime(os.path.join(HERE, f)) > t
+               for f in ("ifc_oracle.c", "ifc_oracle.h", "ifc_oracle_impl.h"))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        for s, T in (("f", C.c_float), ("d", C.c_double)):
+            P = C.c_void_p
+            sig = {
+                "create": (P, [C.POINTER(OrcConfig)]), "destroy": (None, [P]),
+                "field": (C.POINTER(T), [P, C.c_int]), "field_len": (C.c_size_t, [P, C.c_int]),
+                "init_face_vel": (None, [P]), "bc_face_vel": (None, [P]), "mom_link_coef": (None, [P]),
+                "mom_src": (None, [P]), "bc_mom": (None, [P]), "sweep": (C.c_double, [P, C.c_int, C.c_int]),
+                "linear_solve": (C.c_int, [P, C.c_int, C.POINTER(C.c_double)]),
+                "rhie_chow": (None, [P]), "pcorr_link_coef": (None, [P]), "pcorr_src": (C.c_double, [P]),
+                "pin_pcorr": (None, [P]), "update_field": (None, [P, C.POINTER(OrcNorms)]),
+                "outer_iteration": (C.c_int, [P, C.POINTER(OrcNorms)]),
+                "solve": (C.c_int, [P, C.c_int, C.POINTER(OrcNorms)]),
+                "iteration_count": (C.c_int, [P]),
+            }
+            for name, (res, args) in sig.items():
+                fn = getattr(_lib, f"orc_{name}_{s}")
+                fn.restype = res
+                fn.argtypes = args
+    return _lib
+
+
+def make_struct(cfg: dict) -> tuple[OrcConfig, object]:
+    """Fill an OrcConfig from a config dict; returns (struct, keep-alive)."""
+    c = OrcConfig()
+    c.dim = int(cfg["dim"])
+    c.nx, c.ny = int(cfg["nx"]), int(cfg["ny"])
+    c.nz = int(cfg.get("nz", 1)) if c.dim == 3 else 1
+    for k in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax"):
+        setattr(c, k, float(cfg[k]))
+    c.density = float(cfg["density"])
+    c.viscosity = float(cfg["dynamicViscosity"])
+    for f in range(6):
+        c.bc_type[f] = int(cfg["velBC_type"][f])
+        for q in range(3):
+            c.bc_val[f][q] = float(cfg["velBC_val"][f][q])
+    c.num_outer_iter = int(cfg["numOuterIter"])
+    for q, n in enumerate("uvwp"):
+        c.n_iter[q] = int(cfg[f"nIter_{n}"])
+        c.relax[q] = float(cfg[f"relax_{n}"])
+        c.tol[q] = float(cfg[f"tol_{n}"])
+    c.tol_mass = float(cfg["tol_mass"])
+    c.sweep_mode = int(cfg.get("sweep_mode", GS_REDBLACK))
+    c.check_every = int(cfg.get("check_every", 1))
+    c.criterion = int(cfg.get("criterion", CRIT_PER_FIELD))
+    c.pin_pressure = int(cfg.get("pin_pressure", 0))
+    keep = None
+    prof = cfg.get("inlet_profile")
+    if prof is not None:
+        keep = np.ascontiguousarray(prof, dtype=np.float64)
+        c.inlet_profile = keep.ctypes.data_as(C.POINTER(C.c_double))
+    return c, keep
+
+
+class Oracle:
+    """One oracle state (fields, coefficients, running maxima) for one config."""
+
+    def __init__(self, cfg: dict, precision: str = "f"):
+        assert precision in ("f", "d")
+        self.cfg = dict(cfg)
+        self.s = precision
+        self.dtype = np.float32 if precision == "f" else np.float64
+        self._struct, self._keep = make_struct(cfg)
+        self._h = self._fn("create")(C.byref(self._struct))
+        if not self._h:
+            raise MemoryError("oracle allocation failed")
+        self.dim, self.nx, self.ny = self._struct.dim, self._struct.nx, self._struct.ny
+        self.nz = self._struct.nz
+        self.N = self.nx * self.ny * self.nz
+
+    def _fn(self, name):
+        return getattr(lib(), f"orc_{name}_{self.s}")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._fn("destroy")(h)
+            self._h = None
+
+    def field(self, name: str) -> np.ndarray:
+        """Writable numpy view of one oracle array (flat, reference layout)."""
+        q = FIELDS.index(name)
+        n = self._fn("field_len")(self._h, q)
+        ptr = self._fn("field")(self._h, q)
+        return np.ctypeslib.as_array(ptr, shape=(n,))
+
+    def set_fields(self, **arrays):
+        for k, a in arrays.items():
+            dst = self.field(k)
+            dst[:] = np.asarray(a, dtype=self.dtype).ravel()
+
+    # single steps (names follow the reference's Solver methods)
+    def init_face_vel(self): self._fn("init_face_vel")(self._h)
+    def bc_face_vel(self): self._fn("bc_face_vel")(self._h)
+    def mom_link_coef(self): self._fn("mom_link_coef")(self._h)
+    def mom_src(self): self._fn("mom_src")(self._h)
+    def bc_mom(self): self._fn("bc_mom")(self._h)
+    def rhie_chow(self): self._fn("rhie_chow")(self._h)
+    def pcorr_link_coef(self): self._fn("pcorr_link_coef")(self._h)
+    def pcorr_src(self) -> float: return self._fn("pcorr_src")(self._h)
+    def pin_pcorr(self): self._fn("pin_pcorr")(self._h)
+
+    def sweep(self, eq: int, mode: int = GS_REDBLACK) -> float:
+        return self._fn("sweep")(self._h, eq, mode)
+
+    def linear_solve(self, eq: int):
+        norms = (C.c_double * 4096)()
+        n = self._fn("linear_solve")(self._h, eq, norms)
+        return n, np.array(norms[:n])
+
+    def update_field(self) -> dict:
+        nm = OrcNorms()
+        self._fn("update_field")(self._h, C.byref(nm))
+        return nm.as_dict()
+
+    def outer_iteration(self) -> dict:
+        nm = OrcNorms()
+        self._fn("outer_iteration")(self._h, C.byref(nm))
+        return nm.as_dict()
+
+    def solve(self, max_outer: int = 0) -> tuple[int, dict]:
+        nm = OrcNorms()
+        n = self._fn("solve")(self._h, int(max_outer), C.byref(nm))
+        return n, nm.as_dict()
+
+    @property
+    def iterations(self) -> int:
+        return self._fn("iteration_count")(self._h)

@@ -1,0 +1,104 @@
+"""Converged solves on the GPU against the CPU oracle.
+
+Tolerances: the north star's relative L2 <= 1e-4 on converged u, v, w, p
+(p after removing its mean in closed domains, where it is defined only up to a
+constant).  Against the oracle running the same red-black ordering the device
+must agree far tighter (1e-6), and usually bit for bit.
+"""
+import numpy as np
+import pytest
+
+import ifc
+import oracle as O
+from helpers import rel_l2, to_oracle_cfg
+
+pytestmark = pytest.mark.gpu
+
+SOLVE_CASES = {
+    "cavity64": ifc.cavity2d(64),
+    "channel128x32": ifc.channel2d(128, 32),
+    "cavity3d16": ifc.cavity3d(16),
+}
+
+
+def _fields(obj, get, dim, closed):
+    out = {k: get(k).astype(np.float64) for k in (["u", "v", "w"] if dim == 3 else ["u", "v"])}
+    p = get("p").astype(np.float64)
+    out["p"] = p - p.mean() if closed else p
+    return out
+
+
+@pytest.mark.parametrize("name", list(SOLVE_CASES))
+def test_converged_solve(gpu_ok, name):
+    cfg = SOLVE_CASES[name]
+    closed = all(t != ifc.OUTLET for t in cfg["velBC_type"][: 2 * cfg["dim"]])
+    s = ifc.Solver(cfg)
+    st = s.solve()
+    assert st["status"] == ifc.OK and st["converged"], st
+    dev = _fields(s, s.get, cfg["dim"], closed)
+
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    n, nm = o.solve()
+    assert nm["converged"]
+    same = _fields(o, lambda k: o.field(k).copy(), cfg["dim"], closed)
+    assert abs(st["outer_iterations"] - n) <= 2, (st["outer_iterations"], n)
+    for k in dev:
+        assert rel_l2(dev[k], same[k]) < 1e-6, (k, rel_l2(dev[k], same[k]))
+
+    # FP64, lexicographic oracle: the north-star tolerance.
+    o64 = O.Oracle(to_oracle_cfg(dict(cfg, sweep_mode=O.GS_LEX)), "d")
+    o64.solve()
+    ref = _fields(o64, lambda k: o64.field(k).copy(), cfg["dim"], closed)
+    for k in dev:
+        assert rel_l2(dev[k], ref[k]) < 1e-4, (k, rel_l2(dev[k], ref[k]))
+
+
+def test_fp64_build_matches_fp64_oracle(gpu_ok):
+    cfg = dict(ifc.cavity2d(32), precision="d")
+    s = ifc.Solver(cfg)
+    st = s.solve()
+    o = O.Oracle(to_oracle_cfg(cfg), "d")
+    n, nm = o.solve()
+    assert st["converged"] and nm["converged"]
+    for k in ("u", "v"):
+        assert rel_l2(s.get(k), o.field(k)) < 1e-12
+
+
+def test_jacobi_solve(gpu_ok):
+    cfg = dict(ifc.cavity2d(24), linear_solver=ifc.JACOBI, nIter_p=80)
+    s = ifc.Solver(cfg)
+    st = s.solve()
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    n, nm = o.solve()
+    assert st["converged"] and nm["converged"]
+    assert abs(st["outer_iterations"] - n) <= 2
+    for k in ("u", "v"):
+        assert rel_l2(s.get(k), o.field(k)) < 1e-6
+
+
+def test_reference_criterion_and_log(gpu_ok, capfd):
+    """criterion=REFERENCE reproduces src/Solver.cu:237-268 (all norms over the
+    running max of the pressure norm) and the log lines of :270-285."""
+    cfg = dict(ifc.cavity2d(16), criterion=ifc.CRIT_REFERENCE, tol_u=1e-4, tol_v=1e-4, tol_p=1e-4,
+               tol_mass=1e-8, log_level=1)
+    s = ifc.Solver(cfg)
+    st = s.solve()
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    n, nm = o.solve()
+    assert st["converged"] and nm["converged"]
+    assert abs(st["outer_iterations"] - n) <= 1
+    out = capfd.readouterr().out
+    assert out.startswith("iter: 1\npRelNorm : ")
+    assert "ufRelNorm: " in out and "massNorm : " in out and "-" * 60 in out
+
+
+def test_iterate_fixed_count_and_continue(gpu_ok):
+    cfg = ifc.cavity2d(16)
+    s = ifc.Solver(cfg)
+    st = s.iterate(5)
+    assert st["outer_iterations"] == 5 and st["status"] == ifc.OK
+    st = s.iterate(7)
+    assert st["outer_iterations"] == 12
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    o.solve(12)
+    assert rel_l2(s.get("u"), o.field("u")) < 1e-6

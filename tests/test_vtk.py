@@ -1,0 +1,53 @@
+"""VTK writer on host arrays, checked against the byte layout that the
+reference's Solver::writeVTK produces (src/Solver.cu:301-367): std::ostream
+default formatting (%g, 6 significant digits), a space after every value,
+"float" type labels, no newline after the pressure block."""
+import numpy as np
+import pytest
+
+import ifc
+
+
+def expected_vtk(cfg, u, v, w, p, t, dtype):
+    nx, ny = cfg["nx"], cfg["ny"]
+    nz = cfg["nz"] if cfg["dim"] == 3 else 1
+    T = dtype
+
+    def coords(lo, hi, n):
+        lo_t, d = T(lo), (T(hi) - T(lo)) / T(n)
+        return "".join("%g " % float(lo_t + T(i) * d) for i in range(n + 1))
+
+    n = nx * ny * nz
+    s = ["# vtk DataFile Version 3.0\n", "flash 3d grid and solution\n", "ASCII\n",
+         "DATASET RECTILINEAR_GRID\n", f"DIMENSIONS {nx + 1} {ny + 1} {nz + 1}\n",
+         f"X_COORDINATES {nx + 1} float\n", coords(cfg["xmin"], cfg["xmax"], nx), "\n",
+         f"Y_COORDINATES {ny + 1} float\n", coords(cfg["ymin"], cfg["ymax"], ny), "\n",
+         f"Z_COORDINATES {nz + 1} float\n", coords(cfg["zmin"], cfg["zmax"], nz), "\n",
+         f"CELL_DATA {n}\n", "FIELD FieldData 3\n", f"temperature 1 {n} float\n",
+         "".join("%g " % float(x) for x in t), "\n", f"velocity 3 {n} float\n",
+         "".join("%g %g %g " % (float(a), float(b), float(c)) for a, b, c in zip(u, v, w)), "\n",
+         f"pressure 1 {n} float\n", "".join("%g " % float(x) for x in p)]
+    return "".join(s)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+@pytest.mark.parametrize("cfg", [ifc.channel2d(12, 5), ifc.cavity3d(4, nx=4, ny=3, nz=5)])
+def test_vtk_bytes(tmp_path, cfg, prec):
+    cfg = dict(cfg, precision=prec)
+    dt = np.float32 if prec == "f" else np.float64
+    n = cfg["nx"] * cfg["ny"] * (cfg["nz"] if cfg["dim"] == 3 else 1)
+    rng = np.random.default_rng(1)
+    u, v, w, p = (rng.standard_normal(n).astype(dt) * 10.0 ** rng.integers(-6, 6, n) for _ in range(4))
+    u[0] = -0.0
+    t = np.full(n, 273.0, dt)
+    path = str(tmp_path / "out.vtk")
+    ifc.write_vtk_host(cfg, u, v, w, p, t, path)
+    got = open(path).read()
+    assert got == expected_vtk(cfg, u, v, w, p, t, dt)
+
+
+def test_vtk_bad_path():
+    cfg = ifc.cavity2d(4)
+    z = np.zeros(16, np.float32)
+    with pytest.raises(ifc.IfcError):
+        ifc.write_vtk_host(cfg, z, z, z, z, z, "/nonexistent-dir/x.vtk")
