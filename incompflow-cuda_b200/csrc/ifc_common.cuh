@@ -20,7 +20,7 @@ enum { EQ_U = 0, EQ_V = 1, EQ_W = 2, EQ_P = 3 };
 enum { SQ_P = 0, SQ_U, SQ_V, SQ_W, SQ_UF, SQ_VF, SQ_WF, SQ_MASS, SQ_PCSUM, SQ_COUNT };
 
 constexpr int kLogCap = 256;        // log records kept per solve call
-constexpr int kMaxReduce = 8;       // values reduced per kernel
+constexpr int kMaxReduce = 16;      // values reduced per kernel
 
 // Geometry and parameters, evaluated in the solver's scalar type exactly as the
 // reference's constexpr values (include/constants.h:22-28).
@@ -67,6 +67,7 @@ struct Ctl {
     int status;                     // 0 ok, 2 diverged
     int stop[4];                    // inner early-exit flags of this outer iteration
     int sweeps[4];                  // sweeps done in this outer iteration
+    int it_sweeps[4];               // sweeps done in the last finished outer iteration
     long long cell_updates;         // relaxed point updates since the last reset
     double inner_max[4];            // largest RMS sweep change of this outer iteration
     double half_sq[4];              // red-half sum of the sweep in progress

@@ -183,7 +183,11 @@ struct Engine : EngineBase {
         A_(f.uf, nface(0)); A_(f.vf, nface(1)); A_(f.wf, nface(2));
         A_(f.ac, N); A_(f.mc, N * nc); A_(f.pcoef, N * nc);
         A_(f.su, N); A_(f.sv, N); A_(f.sw, N); A_(f.sp, N); A_(f.tmp, 3 * N);
-        A_(partials, (size_t)max_grid * kMaxReduce + 4096 * 8);
+        // One FP64 partial per value and block: the grid-stride kernels use at
+        // most max_grid blocks, the tiled 2D kernels one block per 32x8 tile.
+        const size_t tiles = (size_t)((P.g.nx + 31) / 32) * (size_t)((P.g.ny + 7) / 8) * (size_t)P.g.nz;
+        const size_t max_blocks = tiles > (size_t)max_grid ? tiles : (size_t)max_grid;
+        A_(partials, max_blocks * kMaxReduce);
         A_(ctl, 1);
 #undef A_
         if (c.inlet_profile) {
@@ -199,6 +203,7 @@ struct Engine : EngineBase {
         pin = c.pin_pressure == 1 || (c.pin_pressure < 0 && closed);
         fused = (dim == 2) && fused2d_supported<T>(P.g);
         if (c.sweeps_per_pass > 0) spp_mom = spp_p = c.sweeps_per_pass;
+        if (fused && (rc = prepare_fused()) != IFC_OK) return rc;
         if ((rc = set_uniform(0.0, 0.0, 0.0, 0.0, 273.0)) != IFC_OK) return rc;
         if ((rc = build_graph()) != IFC_OK) return rc;
         return IFC_OK;
@@ -360,6 +365,10 @@ struct Engine : EngineBase {
     template <int DIM>
     void enq_rhie_chow()
     {
+        if (DIM == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+            enq_fused_rc();
+            return;
+        }
         const long long nf = (long long)nface(0) + nface(1) + (DIM == 3 ? (long long)nface(2) : 0);
         k_rhie_chow<T, DIM><<<grid(nf), 256, 0, stream>>>(P, f);
         k_pcorr_src<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl, partials);
@@ -404,7 +413,8 @@ struct Engine : EngineBase {
     template <int DIM>
     void enq_iteration(int use_cond)
     {
-        enq_face_bc<DIM>();
+        // The boundary faces of each iteration are written by the previous
+        // iteration's update kernel; run() applies them before the first.
         enq_mom_solve<DIM>();
         enq_rhie_chow<DIM>();
         enq_pcorr_solve<DIM>();
@@ -420,6 +430,8 @@ struct Engine : EngineBase {
     // Fused 2D path (ifc_fused2d.cuh).
     void enq_fused_mom();
     void enq_fused_pcorr();
+    void enq_fused_rc();
+    int prepare_fused();
 
     int build_graph()
     {
@@ -498,7 +510,7 @@ struct Engine : EngineBase {
         std::memset(st, 0, sizeof(*st));
         st->outer_iterations = ctl_h.it;
         st->converged = ctl_h.converged;
-        for (int q = 0; q < 4; ++q) st->sweeps[q] = ctl_h.sweeps[q];
+        for (int q = 0; q < 4; ++q) st->sweeps[q] = ctl_h.it_sweeps[q];
         st->cell_updates = ctl_h.cell_updates;
         const double *n = ctl_h.norm, *r = ctl_h.rel;
         st->norm_p = n[0]; st->norm_u = n[1]; st->norm_v = n[2]; st->norm_w = n[3];
@@ -525,6 +537,8 @@ struct Engine : EngineBase {
         }
         k_begin<<<1, 1, 0, stream>>>(ctl, n_outer, act, cfg.log_level);
         IFC_CK(cudaEventRecord(ev0, stream));
+        if (dim == 2) enq_face_bc<2>();
+        else enq_face_bc<3>();
         if (exec) {
             IFC_CK(cudaGraphLaunch(exec, stream));
         } else {
@@ -542,9 +556,9 @@ struct Engine : EngineBase {
         last_ms = ms;
         if ((rc = read_ctl()) != IFC_OK) return rc;
         if (cfg.log_level > 0) print_log();
+        last_launches = 2 + (long long)(ctl_h.it - ctl_h.it_begin) * launches_per_iter;
         fill_stats(st);
         int status = IFC_OK;
-        last_launches = (long long)(ctl_h.it - ctl_h.it_begin) * launches_per_iter;
         if (ctl_h.status == 2) status = IFC_DIVERGED;
         else if (act && !ctl_h.converged) status = IFC_NOT_CONVERGED;
         if (st) st->status = status;
@@ -570,10 +584,16 @@ struct Engine : EngineBase {
         switch (stage) {
         case IFC_STAGE_FACE_BC: enq_face_bc<DIM>(); break;
         case IFC_STAGE_MOM_ASSEMBLE: enq_mom_assemble<DIM>(); break;
-        case IFC_STAGE_MOM_SOLVE: enq_mom_solve<DIM>(); break;
+        case IFC_STAGE_MOM_SOLVE:
+            k_reset_inner<<<1, 1, 0, stream>>>(ctl, 7);
+            enq_mom_solve<DIM>();
+            break;
         case IFC_STAGE_RHIE_CHOW: enq_rhie_chow<DIM>(); break;
         case IFC_STAGE_PCORR_COEF: enq_pcorr_coef<DIM>(); break;
-        case IFC_STAGE_PCORR_SOLVE: enq_pcorr_solve<DIM>(); break;
+        case IFC_STAGE_PCORR_SOLVE:
+            k_reset_inner<<<1, 1, 0, stream>>>(ctl, 8);
+            enq_pcorr_solve<DIM>();
+            break;
         case IFC_STAGE_UPDATE:
             k_begin<<<1, 1, 0, stream>>>(ctl, 1, 0, 0);
             enq_update<DIM>(0);

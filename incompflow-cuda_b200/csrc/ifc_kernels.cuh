@@ -22,18 +22,32 @@ __device__ __forceinline__ void reset_inner(Ctl *ctl, int mask)
         }
 }
 
-// Record one finished sweep of equation e (sum of squared changes sq) and
-// apply the inner early-exit rule of src/Solver.cu:955-962.
-__device__ __forceinline__ void finish_sweep(Ctl *ctl, int e, double sq, int N, double tol)
+// Record the sweeps of one pass of equation e (sums of squared changes sq[s],
+// s < ns) and apply the inner early-exit rule of src/Solver.cu:955-962 after
+// each of them; the rule is evaluated only until it first fires.  Run by one
+// thread: the control-block fields are read once, updated in registers and
+// written back once, so the epilogue costs one round trip to L2, not one per
+// field access.
+__device__ __forceinline__ void finish_sweeps(Ctl *ctl, int e, const double *sq, int ns, int N, double tol)
 {
-    double rms = sqrt(sq / (double)N);
     double mx = ctl->inner_max[e];
-    if (rms > mx) mx = rms;
+    int sw = ctl->sweeps[e];
+    long long cu = ctl->cell_updates;
+    bool stop_now = false;
+    for (int s = 0; s < ns; ++s) {
+        if (!stop_now) {
+            const double rms = sqrt(sq[s] / (double)N);
+            if (rms > mx) mx = rms;
+            if (rms / (mx + 1e-20) < tol) stop_now = true;
+        }
+    }
+    sw += ns;
+    cu += (long long)ns * N;
     ctl->inner_max[e] = mx;
-    if (rms / (mx + 1e-20) < tol) ctl->stop[e] = 1;
-    ctl->sweeps[e] += 1;
-    ctl->last_sweep_sq[e] = sq;
-    ctl->cell_updates += N;
+    ctl->sweeps[e] = sw;
+    ctl->cell_updates = cu;
+    if (ns > 0) ctl->last_sweep_sq[e] = sq[ns - 1];
+    if (stop_now) ctl->stop[e] = 1;
 }
 
 // ---- face boundary conditions (+ first-iteration face init) ---------------
@@ -203,7 +217,7 @@ __global__ void k_sweep(Params<T> P, SweepArgs<T, NC> A, Ctl *ctl, double *parti
                 ctl->half_sq[e] = tot[c];
             } else {
                 double s = (A.color == 1 ? ctl->half_sq[e] : 0.0) + tot[c];
-                finish_sweep(ctl, e, s, N, g.tol[e]);
+                finish_sweeps(ctl, e, &s, 1, N, g.tol[e]);
             }
         }
     }
@@ -353,6 +367,18 @@ template <typename T>
 __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, cudaGraphConditionalHandle cond,
                                  int use_cond)
 {
+    // Read every control field this epilogue needs at once (one L2 round
+    // trip), work in registers, write back at the end.
+    const double mass_sq = ctl->sq[SQ_MASS];
+    const int it0 = ctl->it, it_begin = ctl->it_begin, it_stop = ctl->it_stop, act = ctl->act;
+    const int log_level = ctl->log_level, log_n = ctl->log_n;
+    double maxn[8];
+    int sweeps[4];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) maxn[q] = ctl->maxn[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sweeps[q] = ctl->sweeps[q];
+
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const double N = (double)g.N;
     const bool d3 = g.dim == 3;
@@ -364,26 +390,30 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
     n[4] = sqrt(tot[4] / ((double)(nx - 1) * ny * nz));
     n[5] = sqrt(tot[5] / ((double)nx * (ny - 1) * nz));
     n[6] = d3 ? sqrt(tot[6] / ((double)nx * ny * (nz - 1))) : 0.0;
-    n[7] = sqrt(ctl->sq[SQ_MASS] / N);
-    for (int q = 0; q < 7; ++q) ctl->sq[q] = tot[q];
+    n[7] = sqrt(mass_sq / N);
     bool bad = false;
+#pragma unroll
     for (int q = 0; q < 8; ++q) bad = bad || !isfinite(n[q]);
-    const int it = ++ctl->it;
-    if (!bad && it - ctl->it_begin > 1)
-        for (int q = 0; q < 7; ++q) bad = bad || (ctl->maxn[q] > 0.0 && n[q] > 1e6 * ctl->maxn[q]);
+    const int it = it0 + 1;
+    if (!bad && it - it_begin > 1)
+#pragma unroll
+        for (int q = 0; q < 7; ++q) bad = bad || (maxn[q] > 0.0 && n[q] > 1e6 * maxn[q]);
     double rel[7];
     if (g.criterion == 0) {
         // src/Solver.cu:237-256: all relative norms use the running max of the
         // pressure norm.
-        if (n[0] > ctl->maxn[0]) ctl->maxn[0] = n[0];
-        for (int q = 0; q < 7; ++q) rel[q] = n[q] / ctl->maxn[0];
+        if (n[0] > maxn[0]) maxn[0] = n[0];
+#pragma unroll
+        for (int q = 0; q < 7; ++q) rel[q] = n[q] / maxn[0];
     } else {
+#pragma unroll
         for (int q = 0; q < 7; ++q) {
-            if (q == 3 || q == 6) {
-                if (!d3) { rel[q] = 0.0; continue; }
+            if (!d3 && (q == 3 || q == 6)) {
+                rel[q] = 0.0;
+                continue;
             }
-            if (n[q] > ctl->maxn[q]) ctl->maxn[q] = n[q];
-            rel[q] = ctl->maxn[q] > 0.0 ? n[q] / ctl->maxn[q] : 0.0;
+            if (n[q] > maxn[q]) maxn[q] = n[q];
+            rel[q] = maxn[q] > 0.0 ? n[q] / maxn[q] : 0.0;
         }
     }
     // src/Solver.cu:258-268 (p, u, v, uf, vf [, w, wf]) or the mass norm.
@@ -391,21 +421,34 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
                 rel[5] < g.tol[EQ_V];
     if (d3) conv = conv && rel[3] < g.tol[EQ_W] && rel[6] < g.tol[EQ_W];
     conv = conv || n[7] < g.tol_mass;
-    for (int q = 0; q < 8; ++q) ctl->norm[q] = n[q];
+    const int local = it - it_begin;
+    const bool last = it >= it_stop || (act && conv) || bad;
+
+#pragma unroll
+    for (int q = 0; q < 7; ++q) ctl->sq[q] = tot[q];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        ctl->norm[q] = n[q];
+        ctl->maxn[q] = maxn[q];
+    }
+#pragma unroll
     for (int q = 0; q < 7; ++q) ctl->rel[q] = rel[q];
+    ctl->it = it;
     ctl->converged = conv ? 1 : 0;
     if (bad) ctl->status = 2;
-    const int local = it - ctl->it_begin;
-    const bool last = it >= ctl->it_stop || (ctl->act && conv) || bad;
-    if (ctl->log_level > 0 && (local == 1 || local % 1000 == 0 || conv || last)) {
-        int slot = ctl->log_n < kLogCap ? ctl->log_n : kLogCap - 1;
+    if (log_level > 0 && (local == 1 || local % 1000 == 0 || conv || last)) {
+        const int slot = log_n < kLogCap ? log_n : kLogCap - 1;
         LogRec &L = ctl->log[slot];
         L.it = local;
         L.converged = conv;
+#pragma unroll
         for (int q = 0; q < 7; ++q) L.rel[q] = rel[q];
         L.mass = n[7];
-        if (ctl->log_n < kLogCap) ctl->log_n++;
+        if (log_n < kLogCap) ctl->log_n = log_n + 1;
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ctl->it_sweeps[q] = sweeps[q];
+    reset_inner(ctl, 15);
     if (use_cond) cudaGraphSetConditional(cond, last ? 0u : 1u);
 }
 
@@ -426,19 +469,30 @@ __global__ void k_update(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, c
         T L = i > 0 ? f.pc[c - 1] : (g.closed[WEST] ? pc : (T)0);
         T R = i < nx - 1 ? f.pc[c + 1] : (g.closed[EAST] ? pc : (T)0);
         T d = vel_corr(P.d.ru[0], L, R, g.Ax, aC);
-        f.u[c] += d;
+        const T un = f.u[c] + d;
+        f.u[c] = un;
         s[1] += (double)d * (double)d;
+        // Boundary faces of the next outer iteration (kernels.cuh:47-95 with
+        // the corrected velocities, src/Solver.cu:165).
+        if (i == 0) f.uf[(nx + 1) * (j + ny * k)] = face_bc(g, WEST, 0, un, j + ny * k);
+        if (i == nx - 1) f.uf[nx + (nx + 1) * (j + ny * k)] = face_bc(g, EAST, 0, un, j + ny * k);
         L = j > 0 ? f.pc[c - nx] : (g.closed[SOUTH] ? pc : (T)0);
         R = j < ny - 1 ? f.pc[c + nx] : (g.closed[NORTH] ? pc : (T)0);
         d = vel_corr(P.d.ru[1], L, R, g.Ay, aC);
-        f.v[c] += d;
+        const T vn = f.v[c] + d;
+        f.v[c] = vn;
         s[2] += (double)d * (double)d;
+        if (j == 0) f.vf[i + nx * ((ny + 1) * k)] = face_bc(g, SOUTH, 1, vn, 0);
+        if (j == ny - 1) f.vf[i + nx * (ny + (ny + 1) * k)] = face_bc(g, NORTH, 1, vn, 0);
         if (DIM == 3) {
             L = k > 0 ? f.pc[c - pl] : (g.closed[BOTTOM] ? pc : (T)0);
             R = k < nz - 1 ? f.pc[c + pl] : (g.closed[TOP] ? pc : (T)0);
             d = vel_corr(P.d.ru[2], L, R, g.Az, aC);
-            f.w[c] += d;
+            const T wn = f.w[c] + d;
+            f.w[c] = wn;
             s[3] += (double)d * (double)d;
+            if (k == 0) f.wf[c] = face_bc(g, BOTTOM, 2, wn, 0);
+            if (k == nz - 1) f.wf[c + pl] = face_bc(g, TOP, 2, wn, 0);
         }
         if (i >= 1) {
             d = face_corr(P.d.ru[0], f.ac[c - 1], aC, f.pc[c - 1], pc, g.Ax);
@@ -479,6 +533,7 @@ __global__ void k_begin(Ctl *ctl, int n_iter, int act, int log_level)
     ctl->log_level = log_level;
     ctl->cell_updates = 0;
     ctl->counter = 0;
+    reset_inner(ctl, 15);
 }
 
 __global__ void k_reset_inner(Ctl *ctl, int mask) { reset_inner(ctl, mask); }

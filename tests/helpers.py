@@ -6,12 +6,24 @@ import ifc
 import oracle as O
 
 
+def fused_sweeps_per_pass(cfg: dict) -> int:
+    """Sweeps per pass of the fused 2D kernels (the library's default is 4;
+    requests round down to a supported value: 1 2 3 4 5 6 8)."""
+    want = int(cfg.get("sweeps_per_pass", 0)) or 4
+    for k in (8, 6, 5, 4, 3, 2):
+        if want >= k:
+            return k
+    return 1
+
+
 def to_oracle_cfg(cfg: dict) -> dict:
-    """Oracle config for a library config (same keys; red-black sweeps,
-    inner early-exit test after every sweep like the per-step device path)."""
+    """Oracle config for a library config (same keys; red-black sweeps; the
+    inner early-exit rule evaluated at the granularity the device uses: after
+    every pass of the fused 2D kernels, after every sweep otherwise)."""
     c = dict(cfg)
-    c.setdefault("sweep_mode", O.GS_REDBLACK if cfg.get("linear_solver", 0) == 0 else O.JACOBI)
-    c.setdefault("check_every", 1)
+    gs = cfg.get("linear_solver", 0) == 0
+    c.setdefault("sweep_mode", O.GS_REDBLACK if gs else O.JACOBI)
+    c.setdefault("check_every", fused_sweeps_per_pass(cfg) if (gs and cfg["dim"] == 2) else 1)
     c["criterion"] = cfg.get("criterion", O.CRIT_PER_FIELD)
     if "pin_pressure" not in cfg or cfg["pin_pressure"] < 0:
         closed = all(t != ifc.OUTLET for t in cfg["velBC_type"][: 2 * cfg["dim"]])
