@@ -182,6 +182,26 @@ int ifc_time_stage(ifc_solver *h, int stage, int reps, double *ms, int *launches
 /* Norms of the last outer iteration and the running maxima (see ifc_stats). */
 int ifc_get_stats(ifc_solver *h, ifc_stats *stats);
 
+/* Red-black Gauss-Seidel sweeps on caller-owned device buffers, allocating
+ * nothing.  No counterpart in the reference: it exists for callers that cannot
+ * call cudaMalloc -- a program that reserved the whole device for its own pool,
+ * or a time-critical loop that cannot afford cudaFree (it synchronises the
+ * device).  Runs the same sweep kernel as ifc_sweep: coef holds 2*dim+1
+ * planes coef[cell + N*slot] (slots aC,aE,aW,aN,aS[,aT,aB]), src and phi N
+ * cells, all device pointers in the precision given (IFC_FP32 or IFC_FP64);
+ * phi is updated in place by n_sweeps sweeps relaxed by `relax`, with no inner
+ * early exit; sq_norms (optional host array, n_sweeps entries) receives the
+ * FP64 sum of squared changes of each sweep.  stream: cudaStream_t or NULL.
+ * Scratch comes from a fixed 152 KB array inside the library, held on every
+ * GPU that loads it until the process exits.  Grids above 2^26 cells are
+ * rejected with IFC_BAD_ARGUMENT and a message on stderr.  The first call on a
+ * device looks the array's address up (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU (from several streams or threads) race.  Returns when
+ * the sweeps are done. */
+int ifc_rb_sweeps_noalloc(int dim, int nx, int ny, int nz, int precision, const void *coef, const void *src,
+                          void *phi, double relax, int n_sweeps, double *sq_norms, void *stream);
+
 const char *ifc_status_string(int status);
 const char *ifc_last_error(const ifc_solver *h);
 int ifc_abi_version(void);

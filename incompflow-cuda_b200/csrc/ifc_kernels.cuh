@@ -522,7 +522,7 @@ __global__ void k_fill(T *x, long long n, T v)
         x[q] = v;
 }
 
-__global__ void k_begin(Ctl *ctl, int n_iter, int act, int log_level)
+static __global__ void k_begin(Ctl *ctl, int n_iter, int act, int log_level)
 {
     ctl->it_begin = ctl->it;
     ctl->it_stop = ctl->it + n_iter;
@@ -536,6 +536,6 @@ __global__ void k_begin(Ctl *ctl, int n_iter, int act, int log_level)
     reset_inner(ctl, 15);
 }
 
-__global__ void k_reset_inner(Ctl *ctl, int mask) { reset_inner(ctl, mask); }
+static __global__ void k_reset_inner(Ctl *ctl, int mask) { reset_inner(ctl, mask); }
 
 }  // namespace ifc
