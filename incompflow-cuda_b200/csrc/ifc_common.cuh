@@ -125,13 +125,22 @@ __device__ bool grid_reduce(double (&v)[NR], double *partials, Ctl *ctl, double 
     __syncthreads();
     if (!last) return false;
     __threadfence();
+    // All loads first (one round trip to L2 for all values), then the sums.
+    double x[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) x[r] = 0.0;
+    for (int b0 = 0; b0 < (int)gridDim.x; b0 += blockDim.x) {
+        const int b = b0 + threadIdx.x;
+        double y[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) y[r] = b < (int)gridDim.x ? __ldcg(&partials[(size_t)r * gridDim.x + b]) : 0.0;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) x[r] += y[r];
+    }
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
-        double x = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-            x += __ldcg(&partials[(size_t)r * gridDim.x + b]);
-        x = warp_sum(x);
-        if (lane == 0) red[warp][r] = x;
+        const double t = warp_sum(x[r]);
+        if (lane == 0) red[warp][r] = t;
     }
     __syncthreads();
     if (warp == 0) {

@@ -12,7 +12,7 @@
 
 #include "ifc.h"
 #include "ifc_kernels.cuh"
-#include "ifc_fused2d.cuh"
+#include "ifc_persist2d.cuh"
 
 namespace ifc {
 
@@ -105,7 +105,10 @@ struct Engine : EngineBase {
     int dim = 2;
     bool pin = false;
     bool fused = false;               // 2D temporally blocked kernels
-    int spp_mom = 4, spp_p = 4;       // sweeps per pass of the fused kernels
+    int spp_mom = 5, spp_p = 5;       // sweeps per pass of the fused kernels
+    int spp_persist = 5;              // sweeps per pass of the single-launch solve
+    bool persist = false;             // the whole loop runs as one cooperative launch
+    GridBarrier *barrier = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t body_graph = nullptr;
@@ -189,6 +192,7 @@ struct Engine : EngineBase {
         const size_t max_blocks = tiles > (size_t)max_grid ? tiles : (size_t)max_grid;
         A_(partials, max_blocks * kMaxReduce);
         A_(ctl, 1);
+        A_(barrier, 1);
 #undef A_
         if (c.inlet_profile) {
             const size_t n = (size_t)P.g.ny * P.g.nz;
@@ -202,8 +206,9 @@ struct Engine : EngineBase {
         for (int q = 0; q < 2 * dim; ++q) closed = closed && c.vel_bc_type[q] != IFC_OUTLET;
         pin = c.pin_pressure == 1 || (c.pin_pressure < 0 && closed);
         fused = (dim == 2) && fused2d_supported<T>(P.g);
-        if (c.sweeps_per_pass > 0) spp_mom = spp_p = c.sweeps_per_pass;
+        if (c.sweeps_per_pass > 0) spp_mom = spp_p = spp_persist = c.sweeps_per_pass;
         if (fused && (rc = prepare_fused()) != IFC_OK) return rc;
+        if ((rc = prepare_persist()) != IFC_OK) return rc;
         if ((rc = set_uniform(0.0, 0.0, 0.0, 0.0, 273.0)) != IFC_OK) return rc;
         if ((rc = build_graph()) != IFC_OK) return rc;
         return IFC_OK;
@@ -432,6 +437,8 @@ struct Engine : EngineBase {
     void enq_fused_pcorr();
     void enq_fused_rc();
     int prepare_fused();
+    int prepare_persist();
+    int launch_persist();
 
     int build_graph()
     {
@@ -539,7 +546,12 @@ struct Engine : EngineBase {
         IFC_CK(cudaEventRecord(ev0, stream));
         if (dim == 2) enq_face_bc<2>();
         else enq_face_bc<3>();
-        if (exec) {
+        if (persist) {
+            if ((rc = launch_persist()) != IFC_OK) {
+                err = std::string("cooperative launch failed: ") + cudaGetErrorString(cudaGetLastError());
+                return rc;
+            }
+        } else if (exec) {
             IFC_CK(cudaGraphLaunch(exec, stream));
         } else {
             for (int q = 0; q < n_outer; ++q) {
@@ -556,10 +568,13 @@ struct Engine : EngineBase {
         last_ms = ms;
         if ((rc = read_ctl()) != IFC_OK) return rc;
         if (cfg.log_level > 0) print_log();
-        last_launches = 2 + (long long)(ctl_h.it - ctl_h.it_begin) * launches_per_iter;
+        last_launches = persist ? 3 : 2 + (long long)(ctl_h.it - ctl_h.it_begin) * launches_per_iter;
         fill_stats(st);
         int status = IFC_OK;
-        if (ctl_h.status == 2) status = IFC_DIVERGED;
+        if (ctl_h.status == 3) {
+            status = IFC_TIMEOUT;
+            err = "a grid barrier of the single-launch solve timed out";
+        } else if (ctl_h.status == 2) status = IFC_DIVERGED;
         else if (act && !ctl_h.converged) status = IFC_NOT_CONVERGED;
         if (st) st->status = status;
         return status;

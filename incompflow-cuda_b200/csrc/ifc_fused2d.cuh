@@ -53,6 +53,13 @@ __device__ __forceinline__ int colored_cell(int q2, int color, int gx0, int gy0)
     return b * W + a;
 }
 
+// Sweeps of a solve of n sweeps that fall into pass `pass` of KS sweeps each.
+__host__ __device__ __forceinline__ int clamp_sweeps(int n, int pass, int ks)
+{
+    const int r = n - pass * ks;
+    return r < 0 ? 0 : (r > ks ? ks : r);
+}
+
 struct PassArgs {
     int ns[3];      // sweeps of each component in this pass
     int first;      // first pass of the solve (writes aC / starts p' from 0)
@@ -76,6 +83,21 @@ __device__ __forceinline__ void own_cells(int tid, int gx0, int gy0, int nx, int
             }
             cq[c][k] = q;
         }
+}
+
+// Manhattan distance of region cell q from the tile [H, H+TX) x [H, H+TY).
+// After half sweep h of a pass of 2*ns half sweeps only cells within distance
+// 2*ns-1-h of the tile can still influence the tile's final values (each half
+// sweep carries information one cell further), so cells farther out are not
+// updated: the tile's result is unchanged, the redundant halo work shrinks.
+template <int W, int H, int TX, int TY>
+__device__ __forceinline__ int tile_distance(int q)
+{
+    if (q < 0) return 1 << 20;
+    const int a = q % W, b = q / W;
+    const int dx = a < H ? H - a : (a >= H + TX ? a - (H + TX - 1) : 0);
+    const int dy = b < H ? H - b : (b >= H + TY ? b - (H + TY - 1) : 0);
+    return dx + dy;
 }
 
 // ---- momentum: assembly + KS red-black sweeps of u and v -------------------
@@ -152,6 +174,11 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
         for (int s = 0; s < KS; ++s) acc[c][s] = 0.0;
     const T ru = g.relax[EQ_U], rv = g.relax[EQ_V];
 
+    int dq[2][CPT];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) dq[c][k] = tile_distance<W, H, TX, TY>(cq[c][k]);
 #pragma unroll
     for (int s = 0; s < KS; ++s) {
         const bool du = act[0] && s < pa.ns[0];
@@ -159,18 +186,21 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
         if (!du && !dv) break;
 #pragma unroll
         for (int color = 0; color < 2; ++color) {
+            const int hs = 2 * s + color;
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
                 const int q = cq[color][k];
                 if (q < 0) continue;
                 T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
                 T d;
-                if (du) {
+                const bool nu = du && dq[color][k] <= 2 * pa.ns[0] - 1 - hs;
+                const bool nv = dv && dq[color][k] <= 2 * pa.ns[1] - 1 - hs;
+                if (nu) {
                     su[q] = point_update<T, 2>(a7, cbu[color][k], su[q], su[q + 1], su[q - 1], su[q + W], su[q - W],
                                                (T)0, (T)0, ru, d);
                     if (own[color][k]) acc[0][s] += (double)d * (double)d;
                 }
-                if (dv) {
+                if (nv) {
                     sv[q] = point_update<T, 2>(a7, cbv[color][k], sv[q], sv[q + 1], sv[q - 1], sv[q + W], sv[q - W],
                                                (T)0, (T)0, rv, d);
                     if (own[color][k]) acc[1][s] += (double)d * (double)d;
@@ -267,15 +297,21 @@ __global__ void __launch_bounds__(NT) k_pc_pass2d(Params<T> P, Fields<T> f, Ctl 
 #pragma unroll
     for (int s = 0; s < KS; ++s) acc[s] = 0.0;
     const T relax = g.relax[EQ_P];
+    int dq[2][CPT];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) dq[c][k] = tile_distance<W, H, TX, TY>(cq[c][k]);
 #pragma unroll
     for (int s = 0; s < KS; ++s) {
         if (s >= pa.ns[0]) break;
 #pragma unroll
         for (int color = 0; color < 2; ++color) {
+            const int reach = 2 * pa.ns[0] - 1 - (2 * s + color);
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
                 const int q = cq[color][k];
-                if (q < 0) continue;
+                if (q < 0 || dq[color][k] > reach) continue;
                 T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
                 T d;
                 sx[q] = point_update<T, 2>(a7, cb[color][k], sx[q], sx[q + 1], sx[q - 1], sx[q + W], sx[q - W],

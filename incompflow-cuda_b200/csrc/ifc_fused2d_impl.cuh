@@ -79,11 +79,6 @@ static int dispatch_pc(Engine<T> &e, int ks, const PassArgs &pa, bool prepare = 
     }
 }
 
-static inline int clamp_sweeps(int n, int pass, int ks)
-{
-    int r = n - pass * ks;
-    return r < 0 ? 0 : (r > ks ? ks : r);
-}
 
 // Raise the dynamic shared-memory limit of the kernels this handle launches
 // (done once at creation, outside any stream capture).
@@ -139,6 +134,91 @@ void Engine<T>::enq_fused_rc()
 {
     k_rc_mass2d<T><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl, partials);
     ++launches;
+}
+
+}  // namespace ifc
+
+namespace ifc {
+
+// ---- the persistent single-launch 2D solve (ifc_persist2d.cuh) ----
+template <typename T, int KS>
+static int persist_kernel(Engine<T> &e, bool launch, int *capacity)
+{
+    using S = TileShape2D<T>;
+    using R = Region<S::TX, S::TY, 2 * KS>;
+    const size_t smem = (size_t)3 * R::NR * sizeof(T);
+    auto kern = k_simple2d<T, S::TX, S::TY, KS, S::NT>;
+    if (!launch) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return IFC_CUDA_ERROR;
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, S::NT, smem) != cudaSuccess)
+            return IFC_CUDA_ERROR;
+        *capacity = per_sm * e.nsm;
+        return IFC_OK;
+    }
+    const int tiles = ((e.P.g.nx + S::TX - 1) / S::TX) * ((e.P.g.ny + S::TY - 1) / S::TY);
+    PersistArgs pa;
+    pa.n_iter[0] = e.cfg.n_iter_u;
+    pa.n_iter[1] = e.cfg.n_iter_v;
+    pa.n_iter[2] = 0;
+    pa.n_iter[3] = e.cfg.n_iter_p;
+    pa.pin = e.pin ? 1 : 0;
+    void *args[] = {&e.P, &e.f, &e.ctl, &e.partials, &e.barrier, &pa};
+    return cudaLaunchCooperativeKernel((const void *)kern, dim3(tiles), dim3(S::NT), args, smem, e.stream) ==
+                   cudaSuccess
+               ? IFC_OK
+               : IFC_CUDA_ERROR;
+}
+
+template <typename T>
+static int persist_dispatch(Engine<T> &e, int ks, bool launch, int *capacity)
+{
+    switch (ks) {
+    case 2: return persist_kernel<T, 2>(e, launch, capacity);
+    case 3: return persist_kernel<T, 3>(e, launch, capacity);
+    case 4: return persist_kernel<T, 4>(e, launch, capacity);
+    case 5: return persist_kernel<T, 5>(e, launch, capacity);
+    case 6: return persist_kernel<T, 6>(e, launch, capacity);
+    case 8: return persist_kernel<T, 8>(e, launch, capacity);
+    default: return persist_kernel<T, 10>(e, launch, capacity);
+    }
+}
+
+static inline int persist_ks(int want)
+{
+    if (want >= 10) return 10;
+    if (want >= 8) return 8;
+    return want < 2 ? 2 : (want > 6 ? 6 : want);
+}
+
+// Whether the whole loop fits one cooperative launch (one tile per CTA, all
+// CTAs co-resident).
+template <typename T>
+int Engine<T>::prepare_persist()
+{
+    persist = false;
+    if (dim != 2 || !fused || cfg.linear_solver != IFC_GAUSS_SEIDEL) return IFC_OK;
+    int coop = 0, dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return IFC_OK;
+    int capacity = 0;
+    if (persist_dispatch<T>(*this, persist_ks(spp_persist), false, &capacity) != IFC_OK) {
+        cudaGetLastError();
+        return IFC_OK;
+    }
+    using S = TileShape2D<T>;
+    const int tiles = ((P.g.nx + S::TX - 1) / S::TX) * ((P.g.ny + S::TY - 1) / S::TY);
+    persist = tiles <= capacity;
+    return IFC_OK;
+}
+
+template <typename T>
+int Engine<T>::launch_persist()
+{
+    if (cudaMemsetAsync(barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) return IFC_CUDA_ERROR;
+    ++launches;
+    return persist_dispatch<T>(*this, persist_ks(spp_persist), true, nullptr);
 }
 
 }  // namespace ifc

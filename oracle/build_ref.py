@@ -78,6 +78,17 @@ constexpr scalar tol_mass = {f(tol_mass)};
 """
 
 
+def kernel_cases():
+    """Small 2D cases whose kernels the harness ref_kernels.cu runs one by one."""
+    import ifc
+
+    mixed = ifc.channel2d(20, 13, density=3.0, dynamicViscosity=0.05, relax_u=0.7, relax_v=0.6, relax_p=0.3)
+    mixed["velBC_type"] = [ifc.OUTLET, ifc.INLET, ifc.INLET, ifc.WALL, ifc.WALL, ifc.WALL]
+    mixed["velBC_val"] = [[0, 0, 0], [0.3, 0.05, 0], [0.2, -0.1, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]]
+    cav = ifc.cavity2d(17, ny=19, relax_u=0.7, relax_v=0.7, relax_p=0.3)
+    return {"mixed20x13": mixed, "cavity17x19": cav}
+
+
 def cases():
     import ifc
 
@@ -109,11 +120,16 @@ def build(ref_root: str, only=None):
         cmd = NVCC + [f"-I{d}", f"-I{inc}", src, os.path.join(HERE, "ref_bench.cpp"), "-o", exe]
         subprocess.run(cmd, check=True)
         built.append(exe)
+    for name, c in kernel_cases().items():
+        if only and name not in only:
+            continue
+        d = os.path.join(OUT, f"cfg_{name}")
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "config.h"), "w") as fh:
+            fh.write(config_h(c, 1, 0.0, 0.0, 0.0))
         kexe = os.path.join(OUT, f"ref_kernels_{name}")
-        kcmd = NVCC + [f"-I{d}", f"-I{inc}", os.path.join(HERE, "ref_kernels.cu"), "-o", kexe]
-        if os.path.exists(os.path.join(HERE, "ref_kernels.cu")):
-            subprocess.run(kcmd, check=True)
-            built.append(kexe)
+        subprocess.run(NVCC + [f"-I{d}", f"-I{inc}", os.path.join(HERE, "ref_kernels.cu"), "-o", kexe], check=True)
+        built.append(kexe)
     return built
 
 

@@ -13,8 +13,9 @@
 #include <string>
 #include <vector>
 
-#include "Solver.h"
+// The generated case first (see build_ref.py), then the reference's header.
 #include "config.h"
+#include "Solver.h"
 
 int main(int argc, char **argv)
 {

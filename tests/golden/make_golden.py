@@ -1,0 +1,88 @@
+#!/usr/bin/env python
+"""Regenerate the golden fixtures from the reference's own build (run on a GPU
+machine after `python oracle/build_ref.py` has compiled oracle/_ref/).
+
+  python tests/golden/make_golden.py --out DIR
+
+* ref_kernels_<case>.npz: seeded inputs and the outputs of the reference's
+  kernels (include/kernels.cuh) run one by one by oracle/ref_kernels.cu.
+* ref_solve_<case>.npz: u, v, p of the reference's Solver::solve() after a
+  fixed number of outer iterations well past convergence, read back from its
+  VTK output (6 significant digits).
+Copy the files into tests/golden/ to update the fixtures.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.path.join(ROOT, "oracle", "_ref")
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "incompflow-cuda_b200", "python"))
+
+
+def kernel_inputs(cfg: dict, seed: int) -> dict:
+    rng = np.random.default_rng(seed)
+    nx, ny = cfg["nx"], cfg["ny"]
+    n = nx * ny
+    a_nb = -rng.uniform(0.5, 2.0, (4, n))
+    coef = np.concatenate([(-a_nb.sum(0) + rng.uniform(0.1, 1.0, n))[None], a_nb]).ravel()
+    f = lambda k: rng.uniform(-1, 1, k)
+    return {k: v.astype(np.float32) for k, v in dict(
+        u=f(n), v=f(n), p=f(n), pc=f(n), uf=f((nx + 1) * ny), vf=f(nx * (ny + 1)), coef=coef).items()}
+
+
+def run_kernel_case(name: str, cfg: dict, out: str):
+    ins = kernel_inputs(cfg, seed=2024)
+    with tempfile.TemporaryDirectory() as tmp:
+        din, dout = os.path.join(tmp, "in"), os.path.join(tmp, "out")
+        os.makedirs(din)
+        os.makedirs(dout)
+        for k, v in ins.items():
+            v.tofile(os.path.join(din, f"{k}.bin"))
+        subprocess.run([os.path.join(REF, f"ref_kernels_{name}"), din, dout], check=True)
+        res = {f"out_{f[:-4]}": np.fromfile(os.path.join(dout, f), dtype=np.float32) for f in os.listdir(dout)}
+    np.savez_compressed(os.path.join(out, f"ref_kernels_{name}.npz"), **{f"in_{k}": v for k, v in ins.items()}, **res)
+
+
+def read_vtk(path: str, n: int):
+    toks = open(path).read().split()
+    i = toks.index("velocity")
+    vel = np.array(toks[i + 4:i + 4 + 3 * n], dtype=np.float64).reshape(n, 3)
+    i = toks.index("pressure")
+    p = np.array(toks[i + 4:i + 4 + n], dtype=np.float64)
+    return vel[:, 0], vel[:, 1], p
+
+
+def run_solve_case(name: str, n_cells: int, out: str):
+    with tempfile.TemporaryDirectory() as tmp:
+        r = subprocess.run([os.path.join(REF, f"ref_bench_{name}"), "0", "1", f"{name}.vtk"], cwd=tmp,
+                           capture_output=True, text=True, check=True)
+        u, v, p = read_vtk(os.path.join(tmp, "output", f"{name}.vtk"), n_cells)
+    np.savez_compressed(os.path.join(out, f"ref_solve_{name}.npz"), u=u, v=v, p=p, log=np.array(r.stdout[-2000:]))
+
+
+def main():
+    import build_ref
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    for name, cfg in build_ref.kernel_cases().items():
+        run_kernel_case(name, cfg, a.out)
+    for name, (cfg, *_rest) in build_ref.cases().items():
+        if name.startswith("channel512"):
+            continue
+        run_solve_case(name, cfg["nx"] * cfg["ny"], a.out)
+    print("golden fixtures written to", a.out)
+
+
+if __name__ == "__main__":
+    main()

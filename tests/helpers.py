@@ -7,9 +7,9 @@ import oracle as O
 
 
 def fused_sweeps_per_pass(cfg: dict) -> int:
-    """Sweeps per pass of the fused 2D kernels (the library's default is 4;
+    """Sweeps per pass of the fused 2D kernels (the library default is 5;
     requests round down to a supported value: 1 2 3 4 5 6 8)."""
-    want = int(cfg.get("sweeps_per_pass", 0)) or 4
+    want = int(cfg.get("sweeps_per_pass", 0)) or 5
     for k in (8, 6, 5, 4, 3, 2):
         if want >= k:
             return k
