@@ -46,6 +46,7 @@ struct Fields {
     T *mc, *pcoef;                  // materialised coefficient planes (2*dim+1 each)
     T *su, *sv, *sw, *sp;           // momentum sources and p' source (mass imbalance)
     T *tmp;                         // scratch copy for Jacobi sweeps (3*N)
+    T *rac;                         // 1/aC (3D p' sweeps)
 };
 
 struct LogRec {

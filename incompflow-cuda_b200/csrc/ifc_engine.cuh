@@ -13,6 +13,7 @@
 #include "ifc.h"
 #include "ifc_kernels.cuh"
 #include "ifc_persist2d.cuh"
+#include "ifc_fused3d.cuh"
 
 namespace ifc {
 
@@ -185,7 +186,7 @@ struct Engine : EngineBase {
         A_(f.u, N); A_(f.v, N); A_(f.w, N); A_(f.p, N); A_(f.temp, N); A_(f.pc, N);
         A_(f.uf, nface(0)); A_(f.vf, nface(1)); A_(f.wf, nface(2));
         A_(f.ac, N); A_(f.mc, N * nc); A_(f.pcoef, N * nc);
-        A_(f.su, N); A_(f.sv, N); A_(f.sw, N); A_(f.sp, N); A_(f.tmp, 3 * N);
+        A_(f.su, N); A_(f.sv, N); A_(f.sw, N); A_(f.sp, N); A_(f.tmp, 3 * N); A_(f.rac, N);
         // One FP64 partial per value and block: the grid-stride kernels use at
         // most max_grid blocks, the tiled 2D kernels one block per 32x8 tile.
         const size_t tiles = (size_t)((P.g.nx + 31) / 32) * (size_t)((P.g.ny + 7) / 8) * (size_t)P.g.nz;
@@ -359,6 +360,22 @@ struct Engine : EngineBase {
             enq_fused_mom();
             return;
         }
+        if (DIM == 3 && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+            const int ni[3] = {cfg.n_iter_u, cfg.n_iter_v, cfg.n_iter_w};
+            const int nmax = ni[0] > ni[1] ? (ni[0] > ni[2] ? ni[0] : ni[2]) : (ni[1] > ni[2] ? ni[1] : ni[2]);
+            const long long half = (long long)((P.g.nx + 1) / 2) * P.g.ny * P.g.nz;
+            for (int s = 0; s < (nmax > 0 ? nmax : 1); ++s) {
+                Half3D h;
+                for (int c = 0; c < 3; ++c) h.active[c] = s < ni[c];
+                h.first = s == 0;
+                for (int color = 0; color < 2; ++color) {
+                    h.color = color;
+                    k_mom_half3d<T><<<grid(half), 256, 0, stream>>>(P, f, ctl, partials, h);
+                    ++launches;
+                }
+            }
+            return;
+        }
         enq_mom_assemble<DIM>();
         T *phi[3] = {f.u, f.v, f.w};
         T *src[3] = {f.su, f.sv, f.sw};
@@ -392,6 +409,18 @@ struct Engine : EngineBase {
     {
         if (DIM == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
             enq_fused_pcorr();
+        } else if (DIM == 3 && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+            k_reset_inner_p<<<1, 1, 0, stream>>>(ctl);
+            k_recip_ac<T><<<grid(P.g.N), 256, 0, stream>>>(f.ac, f.rac, P.g.N);
+            launches += 2;
+            if (cfg.n_iter_p == 0) cudaMemsetAsync(f.pc, 0, (size_t)P.g.N * sizeof(T), stream);
+            const long long half = (long long)((P.g.nx + 1) / 2) * P.g.ny * P.g.nz;
+            for (int s = 0; s < cfg.n_iter_p; ++s)
+                for (int color = 0; color < 2; ++color) {
+                    const int zm = s == 0 ? (color == 0 ? 1 : 2) : 0;
+                    k_pc_half3d<T><<<grid(half), 256, 0, stream>>>(P, f, f.rac, ctl, partials, color, zm);
+                    ++launches;
+                }
         } else {
             enq_pcorr_coef<DIM>();
             cudaMemsetAsync(f.pc, 0, (size_t)P.g.N * sizeof(T), stream);

@@ -1,0 +1,144 @@
+// ifc_fused3d.cuh -- 3D red-black half sweeps with on-the-fly coefficients.
+//
+// The reference streams 7 coefficient planes per cell and sweep
+// (include/kernels.cuh:926-1005 reading the planes written by :97-334 and
+// :502-540).  Here the momentum half sweep rebuilds the coefficients, the
+// pressure source and the boundary fold-in of each cell from its six face
+// velocities and seven pressures (mom_cell), and sweeps u, v and w together
+// (they share the coefficients); the p' half sweep builds its six links from
+// the reciprocals 1/aC of the cell and its neighbours (kernels.cuh:518-537),
+// stored once per outer iteration.  Same arithmetic as ifc_physics.cuh, so
+// the results are bit-identical to the per-step kernels and the CPU oracle.
+#pragma once
+
+#include "ifc_kernels.cuh"
+
+namespace ifc {
+
+struct Half3D {
+    int color;      // 0 red, 1 black (completes the sweep)
+    int active[3];  // component takes part in this sweep (s < n_iter)
+    int first;      // first sweep of the solve: store aC
+};
+
+template <typename T>
+__device__ __forceinline__ void colored_ijk(long long q, int color, int hx, int ny, int &i, int &j, int &k)
+{
+    const int i2 = (int)(q % hx);
+    const int r = (int)(q / hx);
+    j = r % ny;
+    k = r / ny;
+    i = 2 * i2 + ((color + j + k) & 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mom_half3d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, Half3D h)
+{
+    const Geo<T> &g = P.g;
+    bool act[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) act[c] = h.active[c] && !ctl->stop[c];
+    if (!act[0] && !act[1] && !act[2] && !h.first) return;  // uniform
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
+    const int hx = (nx + 1) / 2;
+    const long long count = (long long)hx * ny * nz;
+    T *phi[3] = {f.u, f.v, f.w};
+    double sq[3] = {0.0, 0.0, 0.0};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count;
+         q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        colored_ijk<T>(q, h.color, hx, ny, i, j, k);
+        if (i >= nx) continue;
+        const int c = i + nx * (j + ny * k);
+        const int fu = i + (nx + 1) * (j + ny * k), fv = i + nx * (j + (ny + 1) * k);
+        T a[7], b[3];
+        mom_cell<T, 3>(P, i, j, k, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], f.wf[c], f.wf[c + pl], f.p[c],
+                       i > 0 ? f.p[c - 1] : (T)0, i < nx - 1 ? f.p[c + 1] : (T)0, j > 0 ? f.p[c - nx] : (T)0,
+                       j < ny - 1 ? f.p[c + nx] : (T)0, k > 0 ? f.p[c - pl] : (T)0, k < nz - 1 ? f.p[c + pl] : (T)0,
+                       a, b);
+        if (h.first) f.ac[c] = a[AC];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            if (!act[m]) continue;
+            const T *o = phi[m];
+            const T pE = i != nx - 1 ? o[c + 1] : (T)0, pW = i != 0 ? o[c - 1] : (T)0;
+            const T pN = j != ny - 1 ? o[c + nx] : (T)0, pS = j != 0 ? o[c - nx] : (T)0;
+            const T pT = k != nz - 1 ? o[c + pl] : (T)0, pB = k != 0 ? o[c - pl] : (T)0;
+            T d;
+            phi[m][c] = point_update<T, 3>(a, b[m], o[c], pE, pW, pN, pS, pT, pB, g.relax[m], d);
+            sq[m] += (double)d * (double)d;
+        }
+    }
+    __shared__ double tot[3];
+    if (grid_reduce<3>(sq, partials, ctl, tot) && threadIdx.x == 0) {
+        for (int m = 0; m < 3; ++m) {
+            if (!act[m]) continue;
+            if (h.color == 0) {
+                ctl->half_sq[m] = tot[m];
+            } else {
+                double s = ctl->half_sq[m] + tot[m];
+                finish_sweeps(ctl, m, &s, 1, N, g.tol[m]);
+            }
+        }
+    }
+}
+
+// 1/aC of every cell, for the p' links (IEEE division, as the reference's 1/aC).
+template <typename T>
+__global__ void k_recip_ac(const T *ac, T *rac, int N)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) rac[c] = (T)1 / ac[c];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_pc_half3d(Params<T> P, Fields<T> f, const T *rac, Ctl *ctl,
+                                                   double *partials, int color, int zero_mode)
+{
+    const Geo<T> &g = P.g;
+    if (ctl->stop[EQ_P]) return;  // uniform
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
+    const int hx = (nx + 1) / 2;
+    const long long count = (long long)hx * ny * nz;
+    double sq[1] = {0.0};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count;
+         q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        colored_ijk<T>(q, color, hx, ny, i, j, k);
+        if (i >= nx) continue;
+        const int c = i + nx * (j + ny * k);
+        const T r = rac[c];
+        T a[7];
+        a[AE] = i < nx - 1 ? (T)(P.d.Kx * (double)(T)(r + rac[c + 1])) : (T)0;
+        a[AW] = i > 0 ? (T)(P.d.Kx * (double)(T)(r + rac[c - 1])) : (T)0;
+        a[AN] = j < ny - 1 ? (T)(P.d.Ky * (double)(T)(r + rac[c + nx])) : (T)0;
+        a[AS] = j > 0 ? (T)(P.d.Ky * (double)(T)(r + rac[c - nx])) : (T)0;
+        a[AT] = k < nz - 1 ? (T)(P.d.Kz * (double)(T)(r + rac[c + pl])) : (T)0;
+        a[AB] = k > 0 ? (T)(P.d.Kz * (double)(T)(r + rac[c - pl])) : (T)0;
+        a[AC] = -(a[AE] + a[AW] + a[AN] + a[AS]);
+        a[AC] += -(a[AT] + a[AB]);
+        const T *o = f.pc;
+        // The solve starts from p' = 0 (src/Solver.cu:193) without clearing the
+        // array: in the first red half every value is 0 (zero_mode 1); in the
+        // first black half the neighbours are the red cells just written and
+        // only the cell itself is still 0 (zero_mode 2).
+        const bool zn = zero_mode == 1;
+        const T pE = (!zn && i != nx - 1) ? o[c + 1] : (T)0, pW = (!zn && i != 0) ? o[c - 1] : (T)0;
+        const T pN = (!zn && j != ny - 1) ? o[c + nx] : (T)0, pS = (!zn && j != 0) ? o[c - nx] : (T)0;
+        const T pT = (!zn && k != nz - 1) ? o[c + pl] : (T)0, pB = (!zn && k != 0) ? o[c - pl] : (T)0;
+        const T pc = zero_mode ? (T)0 : o[c];
+        T d;
+        f.pc[c] = point_update<T, 3>(a, f.sp[c], pc, pE, pW, pN, pS, pT, pB, g.relax[EQ_P], d);
+        sq[0] += (double)d * (double)d;
+    }
+    __shared__ double tot[1];
+    if (grid_reduce<1>(sq, partials, ctl, tot) && threadIdx.x == 0) {
+        if (color == 0) {
+            ctl->half_sq[EQ_P] = tot[0];
+        } else {
+            double s = ctl->half_sq[EQ_P] + tot[0];
+            finish_sweeps(ctl, EQ_P, &s, 1, N, g.tol[EQ_P]);
+        }
+    }
+}
+
+}  // namespace ifc

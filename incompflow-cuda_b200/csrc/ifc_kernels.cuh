@@ -537,5 +537,6 @@ static __global__ void k_begin(Ctl *ctl, int n_iter, int act, int log_level)
 }
 
 static __global__ void k_reset_inner(Ctl *ctl, int mask) { reset_inner(ctl, mask); }
+static __global__ void k_reset_inner_p(Ctl *ctl) { reset_inner(ctl, 8); }
 
 }  // namespace ifc
