@@ -156,6 +156,29 @@ int ifc_write_vtk(ifc_solver *h, const char *path);
 int ifc_write_vtk_host(const ifc_config *cfg, const void *u, const void *v, const void *w,
                        const void *p, const void *temp, const char *path);
 
+/* ---- batched form: many independent 2D cases in one persistent launch ---- */
+typedef struct ifc_batch_result {
+    int status;                       /* IFC_OK (converged), IFC_NOT_CONVERGED, IFC_DIVERGED */
+    int outer_iterations;
+    int converged;
+    int sweeps[4];                    /* u v w p' sweeps of the last outer iteration */
+    double rel_p, rel_u, rel_v, rel_uf, rel_vf, norm_mass;
+} ifc_batch_result;
+
+/* Solves n independent 2D cases (each a full ifc_config: its own grid, fluid,
+ * boundary conditions and iteration counts; all 2D, Gauss-Seidel, one
+ * precision) to convergence or num_outer_iter, in one persistent kernel of
+ * thread-block clusters that take cases from a device queue, relaunched by a
+ * CUDA graph until every case has finished.  Each case runs the same SIMPLE
+ * iteration as ifc_solve with the per-field convergence rule.  results: n
+ * entries.  fields_out (optional): n host pointers, each receiving u, v, p of
+ * its case (3*nx*ny values of the case's precision), or NULL entries.
+ * device_ms (optional): device time of the whole batch.  Device memory is
+ * allocated for the call and freed before it returns.  No counterpart in the
+ * reference (which solves one compiled-in case per executable). */
+int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result *results, void *const *fields_out,
+                    double *device_ms);
+
 /* ---- single steps, for testing one application of each device kernel ---- */
 enum {
     IFC_STAGE_FACE_BC = 0,       /* first iteration: face init; then face BCs (kernels.cuh:10-95) */

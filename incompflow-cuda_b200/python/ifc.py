@@ -66,6 +66,17 @@ class IfcStats(C.Structure):
         return d
 
 
+class IfcBatchResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("outer_iterations", C.c_int), ("converged", C.c_int),
+                ("sweeps", C.c_int * 4)] + [(n, C.c_double) for n in (
+                    "rel_p", "rel_u", "rel_v", "rel_uf", "rel_vf", "norm_mass")]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_ if n != "sweeps"}
+        d["sweeps"] = list(self.sweeps)
+        return d
+
+
 EXPORTS = {
     "ifc_abi_version": (C.c_int, []),
     "ifc_status_string": (C.c_char_p, [C.c_int]),
@@ -87,6 +98,8 @@ EXPORTS = {
     "ifc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(IfcStats)]),
     "ifc_time_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "ifc_last_error": (C.c_char_p, [C.c_void_p]),
+    "ifc_batch_solve": (C.c_int, [C.POINTER(IfcConfig), C.c_int, C.POINTER(IfcBatchResult),
+                                  C.POINTER(C.c_void_p), C.POINTER(C.c_double)]),
 }
 
 _lib = None
@@ -309,3 +322,64 @@ def write_vtk_host(cfg: dict, u, v, w, p, temp, path: str):
     rc = load().ifc_write_vtk_host(C.byref(s), *[a.ctypes.data for a in arrs], path.encode())
     if rc != OK:
         raise IfcError(rc, "write_vtk_host")
+
+
+def batch_solve(cfgs: list, want_fields: bool = True):
+    """Solve independent 2D cases in one persistent launch (ifc_batch_solve).
+    Returns (results, fields, device_ms): per case a result dict and, when
+    want_fields, a dict of u, v, p arrays."""
+    n = len(cfgs)
+    arr = (IfcConfig * n)()
+    keep = []
+    for k, c in enumerate(cfgs):
+        st, kp = make_struct(c)
+        arr[k] = st
+        keep.append(kp)
+    res = (IfcBatchResult * n)()
+    outs = []
+    ptrs = (C.c_void_p * n)()
+    for k, c in enumerate(cfgs):
+        dt = np.float64 if arr[k].precision == 1 else np.float32
+        buf = np.empty(3 * c["nx"] * c["ny"], dtype=dt) if want_fields else None
+        outs.append(buf)
+        ptrs[k] = buf.ctypes.data if want_fields else None
+    ms = C.c_double()
+    rc = load().ifc_batch_solve(arr, n, res, ptrs, C.byref(ms))
+    if rc != OK:
+        raise IfcError(rc, "batch_solve")
+    fields = []
+    for k, c in enumerate(cfgs):
+        if want_fields:
+            m = c["nx"] * c["ny"]
+            fields.append({"u": outs[k][:m], "v": outs[k][m:2 * m], "p": outs[k][2 * m:]})
+        else:
+            fields.append(None)
+    return [r.as_dict() for r in res], fields, ms.value
+
+
+def batch_cases(n: int = 256, seed: int = 0, sizes=(32, 64, 96, 128, 160, 192, 224, 256)) -> list:
+    """The batched workload: n lid-driven cavities on the unit square, nx and ny
+    drawn uniformly from `sizes`, Re log-uniform in [10, 1000] (mu = 1/Re,
+    rho = 1, lid speed 1), solver settings of the 2D cavity."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx, ny = int(rng.choice(sizes)), int(rng.choice(sizes))
+        re = float(10 ** rng.uniform(1, 3))
+        out.append(cavity2d(nx, re=re, ny=ny))
+    return out
+
+
+def shard_cases(weights: list, rank: int, world: int) -> list:
+    """Indices of the cases rank `rank` of `world` solves: a greedy
+    longest-first split of the case weights (cells x expected iterations) over
+    the ranks, identical on every rank, no communication needed."""
+    order = sorted(range(len(weights)), key=lambda i: (-weights[i], i))
+    load_ = [0.0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (load_[q], q))
+        load_[r] += weights[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)

@@ -1,0 +1,79 @@
+"""The batched form (ifc_batch_solve): many independent 2D cases of uneven
+size, Reynolds number and boundary type in one persistent launch, each checked
+against the CPU oracle run on its own (same red-black ordering, inner
+early-exit rule after every sweep).  Tolerance: relative L2 1e-6 against the
+oracle with the same ordering (FP64 norms summed in a different order can move
+a convergence decision by one iteration), and the north star's 1e-4 against
+the FP64 lexicographic oracle."""
+import numpy as np
+import pytest
+
+import ifc
+import oracle as O
+from helpers import rel_l2, to_oracle_cfg
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_cases():
+    cases = [ifc.cavity2d(16, re=50.0, ny=24), ifc.cavity2d(32, re=400.0), ifc.cavity2d(24, re=1000.0, ny=9),
+             ifc.channel2d(40, 12), ifc.cavity2d(8, re=10.0, ny=33)]
+    for c in cases:
+        c["numOuterIter"] = 3000
+    return cases
+
+
+def oracle_fields(cfg, sweep_mode=O.GS_REDBLACK, prec="f"):
+    o = O.Oracle(to_oracle_cfg(dict(cfg, sweep_mode=sweep_mode, check_every=1)), prec)
+    n, nm = o.solve()
+    p = o.field("p").astype(np.float64)
+    return n, nm, {"u": o.field("u").copy(), "v": o.field("v").copy(), "p": p}
+
+
+def test_batch_matches_oracle(gpu_ok):
+    cases = mixed_cases()
+    res, fields, ms = ifc.batch_solve(cases)
+    assert ms > 0
+    for c, r, f in zip(cases, res, fields):
+        n, nm, ref = oracle_fields(c)
+        assert r["converged"] == nm["converged"] == 1, (r, nm)
+        assert abs(r["outer_iterations"] - n) <= 1, (r["outer_iterations"], n)
+        closed = all(t != ifc.OUTLET for t in c["velBC_type"][:4])
+        for k in ("u", "v", "p"):
+            a, b = f[k].astype(np.float64), ref[k]
+            if k == "p" and closed:
+                a, b = a - a.mean(), b - b.mean()
+            assert rel_l2(a, b) < 1e-6, (c["nx"], c["ny"], k, rel_l2(a, b))
+
+
+def test_batch_is_deterministic_and_order_independent(gpu_ok):
+    cases = mixed_cases()
+    r1, f1, _ = ifc.batch_solve(cases)
+    r2, f2, _ = ifc.batch_solve(list(reversed(cases)))
+    for a, b in zip(f1, reversed(f2)):
+        for k in ("u", "v", "p"):
+            assert np.array_equal(a[k], b[k])
+    assert [x["outer_iterations"] for x in r1] == [x["outer_iterations"] for x in reversed(r2)]
+
+
+def test_batch_case_against_fp64_oracle(gpu_ok):
+    c = ifc.cavity2d(32, re=100.0)
+    res, fields, _ = ifc.batch_solve([c])
+    _, _, ref = oracle_fields(c, O.GS_LEX, "d")
+    for k in ("u", "v", "p"):
+        a, b = fields[0][k].astype(np.float64), ref[k]
+        if k == "p":
+            a, b = a - a.mean(), b - b.mean()
+        assert rel_l2(a, b) < 1e-4
+
+
+def test_batch_rejects_3d_and_mixed_precision():
+    import ctypes as C
+    cfgs = [ifc.cavity3d(8), ifc.cavity2d(8)]
+    arr = (ifc.IfcConfig * 2)()
+    keep = []
+    for k, c in enumerate(cfgs):
+        arr[k], kp = ifc.make_struct(c)
+        keep.append(kp)
+    res = (ifc.IfcBatchResult * 2)()
+    assert ifc.load().ifc_batch_solve(arr, 2, res, None, None) == ifc.UNSUPPORTED
