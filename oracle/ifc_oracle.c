@@ -20,3 +20,8 @@
 #include "ifc_oracle_impl.h"
 #undef T
 #undef S
+
+/* Reverse pass of one outer iteration (FP64, 2D), see ifc_adjoint_impl.h. */
+#include "ifc_adjoint_impl.h"
+
+void orc_set_iteration_count_d(orc_state_d *s, int it) { s->it = it; }

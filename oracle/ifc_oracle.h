@@ -106,6 +106,15 @@ enum {
 ORC_DECLARE(float, f)
 ORC_DECLARE(double, d)
 
+/* Reverse pass of one SIMPLE outer iteration at a fixed point (2D, FP64):
+ * given a seed on the outputs (u, v, p, uf, vf; boundary-face entries ignored)
+ * returns G_x^T seed (same layout, boundary faces 0), G_theta^T seed (west
+ * inlet rows, ny values; needs an inlet profile) and G_mu^T seed. */
+int orc_adjoint_apply_d(orc_state_d *s, const double *lu_in, const double *lv_in, const double *lp_in,
+                        const double *luf_in, const double *lvf_in, double *lu_out, double *lv_out, double *lp_out,
+                        double *luf_out, double *lvf_out, double *ltheta, double *lmu);
+void orc_set_iteration_count_d(orc_state_d *s, int it);
+
 #ifdef __cplusplus
 }
 #endif

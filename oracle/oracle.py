@@ -61,7 +61,7 @@ def build(force: bool = False) -> str:
 def _stale() -> bool:
     t = os.path.getmtime(LIB_PATH)
     return any(os.path.getmtime(os.path.join(HERE, f)) > t
-               for f in ("ifc_oracle.c", "ifc_oracle.h", "ifc_oracle_impl.h"))
+               for f in ("ifc_oracle.c", "ifc_oracle.h", "ifc_oracle_impl.h", "ifc_adjoint_impl.h"))
 
 
 _lib = None
@@ -89,6 +89,11 @@ def lib():
                 fn = getattr(_lib, f"orc_{name}_{s}")
                 fn.restype = res
                 fn.argtypes = args
+        PD = C.POINTER(C.c_double)
+        _lib.orc_adjoint_apply_d.restype = C.c_int
+        _lib.orc_adjoint_apply_d.argtypes = [C.c_void_p] + [PD] * 12
+        _lib.orc_set_iteration_count_d.restype = None
+        _lib.orc_set_iteration_count_d.argtypes = [C.c_void_p, C.c_int]
     return _lib
 
 
@@ -198,3 +203,65 @@ class Oracle:
     @property
     def iterations(self) -> int:
         return self._fn("iteration_count")(self._h)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class AdjointOracle(Oracle):
+    """FP64 oracle with the reverse pass of one outer iteration
+    (orc_adjoint_apply_d) and the adjoint fixed-point solve built on it."""
+
+    def __init__(self, cfg: dict):
+        super().__init__(cfg, "d")
+
+    def state_sizes(self):
+        nx, ny = self.nx, self.ny
+        return {"u": nx * ny, "v": nx * ny, "p": nx * ny, "uf": (nx + 1) * ny, "vf": nx * (ny + 1)}
+
+    def apply_transpose(self, seed: dict):
+        """G_x^T seed, G_theta^T seed, G_mu^T seed at the current (fixed-point) state."""
+        sz = self.state_sizes()
+        ins = {k: np.ascontiguousarray(seed[k], dtype=np.float64) for k in sz}
+        outs = {k: np.zeros(n) for k, n in sz.items()}
+        lth = np.zeros(self.ny)
+        lmu = C.c_double()
+        rc = lib().orc_adjoint_apply_d(self._h, *[_ptr(ins[k]) for k in ("u", "v", "p", "uf", "vf")],
+                                       *[_ptr(outs[k]) for k in ("u", "v", "p", "uf", "vf")], _ptr(lth),
+                                       C.byref(lmu))
+        assert rc == 0
+        return outs, lth, lmu.value
+
+    def set_iteration_count(self, it: int):
+        lib().orc_set_iteration_count_d(self._h, it)
+
+    def objective_seed(self):
+        """dJ/dx of J = mean p over the first cell column - mean over the last."""
+        nx, ny = self.nx, self.ny
+        sz = self.state_sizes()
+        seed = {k: np.zeros(n) for k, n in sz.items()}
+        p = seed["p"].reshape(ny, nx)
+        p[:, 0] = 1.0 / ny
+        p[:, -1] = -1.0 / ny
+        return seed
+
+    def objective(self) -> float:
+        p = self.field("p").reshape(self.ny, self.nx)
+        return float(p[:, 0].mean() - p[:, -1].mean())
+
+    def adjoint_gradient(self, max_iter: int = 100000, tol: float = 1e-12):
+        """Fixed-point adjoint lambda = G_x^T lambda + dJ/dx; returns
+        (dJ/dtheta, dJ/dmu, iterations)."""
+        jx = self.objective_seed()
+        lam = {k: v.copy() for k, v in jx.items()}
+        for it in range(1, max_iter + 1):
+            out, lth, lmu = self.apply_transpose(lam)
+            new = {k: out[k] + jx[k] for k in lam}
+            delta = max(np.abs(new[k] - lam[k]).max() for k in lam)
+            scale = max(np.abs(new[k]).max() for k in lam)
+            lam = new
+            if delta <= tol * scale:
+                break
+        out, lth, lmu = self.apply_transpose(lam)
+        return lth, lmu, it
