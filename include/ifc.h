@@ -179,6 +179,50 @@ typedef struct ifc_batch_result {
 int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result *results, void *const *fields_out,
                     double *device_ms);
 
+/* ---- differentiation form: discrete adjoint of the converged 2D solve ---- */
+/* Objectives of ifc_adjoint. */
+enum {
+    IFC_OBJ_PRESSURE_DROP = 0,        /* J = mean p of the first cell column - mean of the last */
+    IFC_OBJ_CUSTOM = 1                /* dJ/du, dJ/dv, dJ/dp given by the caller */
+};
+
+typedef struct ifc_adjoint_result {
+    int status;
+    int iterations;                   /* adjoint fixed-point iterations (reverse passes) */
+    int converged;
+    double residual;                  /* last max|lambda_new - lambda| / max|lambda_new| */
+    double objective;                 /* J at the current state (IFC_OBJ_PRESSURE_DROP), else NaN */
+    double dJ_dmu;                    /* gradient with respect to the dynamic viscosity */
+    double device_ms;                 /* device time of the whole call (CUDA events) */
+    long long kernel_launches;
+} ifc_adjoint_result;
+
+/* Gradient of an objective J(u, v, p) of the converged state with respect to
+ * the west-inlet velocity of every boundary row (theta, ny values: the
+ * inlet_profile entries, or the uniform inlet value per row) and the dynamic
+ * viscosity, by the discrete adjoint of the SIMPLE outer iteration: the
+ * adjoint lambda = G_x^T lambda + dJ/dx is iterated from lambda = dJ/dx to
+ * relative change `tol` (at most max_iter reverse passes), and
+ * dJ/dtheta = G_theta^T lambda, dJ/dmu = G_mu^T lambda.  The linearisation is
+ * taken at the handle's current fields (solve first); all adjoint arithmetic
+ * is FP64 for either precision of the handle.  dJ_du/dJ_dv/dJ_dp: host arrays
+ * of nx*ny doubles (NULL = 0), read with IFC_OBJ_CUSTOM only.  dJ_dtheta:
+ * host array of ny doubles (zeros unless the west face is an inlet).  2D and
+ * red-black Gauss-Seidel only (IFC_UNSUPPORTED otherwise).  Returns
+ * IFC_NOT_CONVERGED when max_iter passes did not reach tol (the gradient of
+ * the last iterate is still returned).  No counterpart in the reference. */
+int ifc_adjoint(ifc_solver *h, int objective, const double *dJ_du, const double *dJ_dv, const double *dJ_dp,
+                int max_iter, double tol, double *dJ_dtheta, ifc_adjoint_result *result);
+
+/* One reverse pass at the current fields: out = G_x^T lambda (u, v, p: nx*ny;
+ * uf: (nx+1)*ny; vf: nx*(ny+1); boundary-face entries of lambda are ignored
+ * and those of out are 0), dJ_dtheta = G_theta^T lambda (ny), *dJ_dmu =
+ * G_mu^T lambda.  All host arrays of doubles.  For testing the adjoint
+ * operator against a transposition of the forward iteration. */
+int ifc_adjoint_apply(ifc_solver *h, const double *lam_u, const double *lam_v, const double *lam_p,
+                      const double *lam_uf, const double *lam_vf, double *out_u, double *out_v, double *out_p,
+                      double *out_uf, double *out_vf, double *dJ_dtheta, double *dJ_dmu);
+
 /* ---- single steps, for testing one application of each device kernel ---- */
 enum {
     IFC_STAGE_FACE_BC = 0,       /* first iteration: face init; then face BCs (kernels.cuh:10-95) */

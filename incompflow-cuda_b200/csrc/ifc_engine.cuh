@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "ifc.h"
+#include "ifc_adjoint.h"
 #include "ifc_kernels.cuh"
 #include "ifc_persist2d.cuh"
 #include "ifc_fused3d.cuh"
@@ -29,6 +30,7 @@ struct EngineBase {
     virtual int sweep(int eq, int n, double *sq) = 0;
     virtual int stats(ifc_stats *st) = 0;
     virtual int time_stage(int stage, int reps, double *ms, int *launches) = 0;
+    virtual int adjoint(const AdjointReq &rq, ifc_adjoint_result *res) = 0;
     std::string err;
 };
 
@@ -122,9 +124,11 @@ struct Engine : EngineBase {
     long long launches = 0;           // kernels enqueued (counted by the enq_* helpers)
     long long launches_per_iter = 0;  // kernels in one captured outer iteration
     long long last_launches = 0;
+    AdjointCtx *adj = nullptr;        // discrete-adjoint buffers and graphs (first ifc_adjoint call)
 
     ~Engine() override
     {
+        adjoint_free(adj);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (body_exec) cudaGraphExecDestroy(body_exec);
@@ -688,6 +692,14 @@ struct Engine : EngineBase {
             if (sq) sq[s] = ctl_h.last_sweep_sq[eq];
         }
         return IFC_OK;
+    }
+
+    int adjoint(const AdjointReq &rq0, ifc_adjoint_result *res) override
+    {
+        AdjointReq rq = rq0;
+        rq.pin = pin ? 1 : 0;
+        IFC_CK(cudaStreamSynchronize(stream));
+        return adjoint_run<T>(adj, cfg, make_params<double>(cfg), f, inlet_d, stream, rq, res, err);
     }
 
     int stats(ifc_stats *st) override

@@ -217,6 +217,52 @@ int ifc_time_stage(ifc_solver *h, int stage, int reps, double *ms, int *launches
     IFC_END(h)
 }
 
+int ifc_adjoint(ifc_solver *h, int objective, const double *dJ_du, const double *dJ_dv, const double *dJ_dp,
+                int max_iter, double tol, double *dJ_dtheta, ifc_adjoint_result *result)
+{
+    if (objective != IFC_OBJ_PRESSURE_DROP && objective != IFC_OBJ_CUSTOM) return IFC_BAD_ARGUMENT;
+    if (max_iter < 1 || !(tol >= 0.0)) return IFC_BAD_ARGUMENT;
+    IFC_GUARD(h)
+    ifc::AdjointReq rq;
+    std::memset(&rq, 0, sizeof(rq));
+    rq.mode = 0;
+    rq.objective = objective;
+    rq.seed[0] = dJ_du;
+    rq.seed[1] = dJ_dv;
+    rq.seed[2] = dJ_dp;
+    rq.max_iter = max_iter;
+    rq.tol = tol;
+    rq.dtheta = dJ_dtheta;
+    ifc_adjoint_result r;
+    std::memset(&r, 0, sizeof(r));
+    const int rc = h->eng->adjoint(rq, &r);
+    r.status = rc;
+    if (result) *result = r;
+    return rc;
+    IFC_END(h)
+}
+
+int ifc_adjoint_apply(ifc_solver *h, const double *lam_u, const double *lam_v, const double *lam_p,
+                      const double *lam_uf, const double *lam_vf, double *out_u, double *out_v, double *out_p,
+                      double *out_uf, double *out_vf, double *dJ_dtheta, double *dJ_dmu)
+{
+    IFC_GUARD(h)
+    ifc::AdjointReq rq;
+    std::memset(&rq, 0, sizeof(rq));
+    rq.mode = 1;
+    const double *in[5] = {lam_u, lam_v, lam_p, lam_uf, lam_vf};
+    double *out[5] = {out_u, out_v, out_p, out_uf, out_vf};
+    for (int q = 0; q < 5; ++q) {
+        rq.seed[q] = in[q];
+        rq.out[q] = out[q];
+    }
+    rq.max_iter = 1;
+    rq.dtheta = dJ_dtheta;
+    rq.dmu = dJ_dmu;
+    return h->eng->adjoint(rq, nullptr);
+    IFC_END(h)
+}
+
 int ifc_get_stats(ifc_solver *h, ifc_stats *stats)
 {
     IFC_GUARD(h)

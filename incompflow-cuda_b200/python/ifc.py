@@ -77,6 +77,18 @@ class IfcBatchResult(C.Structure):
         return d
 
 
+class IfcAdjointResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("converged", C.c_int)] + [
+        (n, C.c_double) for n in ("residual", "objective", "dJ_dmu", "device_ms")] + [
+        ("kernel_launches", C.c_longlong)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+OBJ_PRESSURE_DROP, OBJ_CUSTOM = 0, 1
+_DP = C.POINTER(C.c_double)
+
 EXPORTS = {
     "ifc_abi_version": (C.c_int, []),
     "ifc_status_string": (C.c_char_p, [C.c_int]),
@@ -100,7 +112,14 @@ EXPORTS = {
     "ifc_last_error": (C.c_char_p, [C.c_void_p]),
     "ifc_batch_solve": (C.c_int, [C.POINTER(IfcConfig), C.c_int, C.POINTER(IfcBatchResult),
                                   C.POINTER(C.c_void_p), C.POINTER(C.c_double)]),
+    "ifc_adjoint": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, C.c_int, C.c_double, _DP,
+                              C.POINTER(IfcAdjointResult)]),
+    "ifc_adjoint_apply": (C.c_int, [C.c_void_p] + [_DP] * 12),
 }
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(_DP)
 
 _lib = None
 
@@ -312,6 +331,35 @@ class Solver:
 
     def write_vtk(self, path: str):
         self._check(load().ifc_write_vtk(self._h, path.encode()), "write_vtk")
+
+    def adjoint(self, objective: int = OBJ_PRESSURE_DROP, dJ_du=None, dJ_dv=None, dJ_dp=None,
+                max_iter: int = 200000, tol: float = 1e-10) -> tuple[np.ndarray, dict]:
+        """Discrete-adjoint gradient at the current state: (dJ/dtheta per inlet
+        row, result dict with dJ_dmu, objective, iterations, device_ms)."""
+        seeds = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (dJ_du, dJ_dv, dJ_dp)]
+        dth = np.zeros(self.ny)
+        r = IfcAdjointResult()
+        self._check(load().ifc_adjoint(self._h, objective, *[_dptr(a) for a in seeds], int(max_iter), float(tol),
+                                       _dptr(dth), C.byref(r)), "adjoint", allow=(OK, NOT_CONVERGED))
+        return dth, r.as_dict()
+
+    def adjoint_apply(self, lam: dict) -> tuple[dict, np.ndarray, float]:
+        """One reverse pass: (G_x^T lam, G_theta^T lam, G_mu^T lam); lam and the
+        result have keys u v p uf vf (FP64)."""
+        nx, ny = self.nx, self.ny
+        sizes = {"u": nx * ny, "v": nx * ny, "p": nx * ny, "uf": (nx + 1) * ny, "vf": nx * (ny + 1)}
+        ins = {k: np.ascontiguousarray(lam[k], dtype=np.float64) for k in sizes}
+        for k, n in sizes.items():
+            if ins[k].size != n:
+                raise ValueError(f"lam[{k}] has {ins[k].size} values, expected {n}")
+        outs = {k: np.zeros(n) for k, n in sizes.items()}
+        dth = np.zeros(ny)
+        dmu = C.c_double()
+        keys = ("u", "v", "p", "uf", "vf")
+        self._check(load().ifc_adjoint_apply(self._h, *[_dptr(ins[k]) for k in keys],
+                                             *[_dptr(outs[k]) for k in keys], _dptr(dth), C.byref(dmu)),
+                    "adjoint_apply")
+        return outs, dth, dmu.value
 
 
 def write_vtk_host(cfg: dict, u, v, w, p, temp, path: str):
