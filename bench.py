@@ -53,6 +53,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--form", default="plain", choices=["plain", "adjoint"],
+                    help="plain: the headline throughput line; adjoint: the differentiation form")
+    ap.add_argument("--profiles", type=int, default=32, help="adjoint form: seeded inlet profiles")
+    ap.add_argument("--fd-profiles", type=int, default=1,
+                    help="adjoint form: profiles whose 65 parameters are checked by central differences")
+    ap.add_argument("--fd-iters", type=int, default=3000,
+                    help="adjoint form: outer iterations of each warm-started FP64 finite-difference solve")
     return ap.parse_args()
 
 
@@ -296,6 +303,159 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+ADJ_WORKLOAD = "channel2d_256x64_adjoint"
+
+
+def adjoint_profile(k: int, ny: int = 64):
+    import numpy as np
+
+    return 0.001 + np.random.default_rng(1000 + k).normal(0.0, 1e-4, ny)
+
+
+def run_adjoint(args):
+    """Differentiation form: for each seeded inlet profile theta (64 values,
+    0.001 m/s + N(0, 1e-4)) an FP32 primal solve of the 256 x 64 channel to
+    the standard per-field criterion 1e-5, then the FP64 discrete adjoint
+    (tol 1e-8) giving dJ/dtheta and dJ/dmu of J = inlet-minus-outlet mean
+    pressure drop.  The metric is adjoint device time / primal device time.
+    A second gradient is taken after POLISH further primal iterations (its
+    error shows how much of the first one's is the primal's stopping point).
+    The first --fd-profiles profiles are checked against central finite
+    differences (relative step 1e-3) of FP64 solves warm-started from the
+    converged FP64 state, for all 65 parameters (two host threads, each with
+    its own handle and stream)."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import ifc
+
+    POLISH = 300
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    nx, ny = 256, 64
+    base_cfg = ifc.channel2d(nx, ny, inlet_profile=adjoint_profile(0))
+    s32 = ifc.Solver(base_cfg)
+    # warm-up: one untimed primal + adjoint
+    s32.solve()
+    s32.adjoint(tol=1e-8)
+    rows = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(args.profiles):
+        theta = adjoint_profile(k, ny)
+        t0 = time.perf_counter()
+        s32.set_inlet_profile(theta)
+        s32.set_uniform()
+        st = s32.solve()
+        dth, res = s32.adjoint(tol=1e-8)
+        wall = time.perf_counter() - t0
+        stp = s32.iterate(POLISH)
+        dth_p, res_p = s32.adjoint(tol=1e-8)
+        rows.append({"theta": theta, "primal_ms": st["device_ms"], "primal_its": st["outer_iterations"],
+                     "primal_converged": st["converged"], "adj_ms": res["device_ms"], "adj_its": res["iterations"],
+                     "adj_converged": res["converged"], "dth": dth, "dmu": res["dJ_dmu"], "J": res["objective"],
+                     "wall_ms": wall * 1e3, "launches": st["kernel_launches"] + res["kernel_launches"],
+                     "polish_ms": stp["device_ms"], "dth_p": dth_p, "dmu_p": res_p["dJ_dmu"]})
+    clk = clocks.stop()
+
+    mu = base_cfg["dynamicViscosity"]
+    keys = ("u", "v", "p", "uf", "vf")
+
+    def J_of(sol):
+        p = sol.get("p").reshape(ny, nx)
+        return float(p[:, 0].mean() - p[:, -1].mean())
+
+    def run_from(sol, base):
+        for f, a in base.items():
+            sol.set(f, a)
+        sol.iterate(args.fd_iters)
+        return J_of(sol)
+
+    fd_rows = []
+    t_fd = time.perf_counter()
+    for k in range(min(args.fd_profiles, args.profiles)):
+        theta = rows[k]["theta"]
+        c64 = dict(base_cfg, precision="d", inlet_profile=theta)
+        s64 = ifc.Solver(c64)
+        s64.solve()
+        s64.iterate(4000)
+        base = {f: s64.get(f) for f in keys}
+        s64.close()
+        fd = np.empty(ny)
+        fdmu = [0.0]
+
+        def worker(js, with_mu):
+            sol = ifc.Solver(c64)
+            for j in js:
+                h = 1e-3 * theta[j]
+                Js = []
+                for sgn in (1.0, -1.0):
+                    tt = theta.copy()
+                    tt[j] += sgn * h
+                    sol.set_inlet_profile(tt)
+                    Js.append(run_from(sol, base))
+                fd[j] = (Js[0] - Js[1]) / (2 * h)
+            sol.close()
+            if with_mu:
+                h = 1e-3 * mu
+                Jm = []
+                for sgn in (1.0, -1.0):
+                    sm = ifc.Solver(dict(c64, dynamicViscosity=mu + sgn * h))
+                    Jm.append(run_from(sm, base))
+                    sm.close()
+                fdmu[0] = (Jm[0] - Jm[1]) / (2 * h)
+
+        th = [threading.Thread(target=worker, args=(list(range(0, ny, 2)), True)),
+              threading.Thread(target=worker, args=(list(range(1, ny, 2)), False))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        rec = {"profile": k}
+        for tag, dth, dmu in (("", rows[k]["dth"], rows[k]["dmu"]), ("polished_", rows[k]["dth_p"], rows[k]["dmu_p"])):
+            rec[tag + "max_rel_err_theta"] = float((np.abs(dth - fd) / np.abs(fd)).max())
+            rec[tag + "rel_err_mu"] = float(abs(dmu - fdmu[0]) / abs(fdmu[0]))
+        fd_rows.append(rec)
+    t_fd = time.perf_counter() - t_fd
+    s32.close()
+
+    pm = np.array([r["primal_ms"] for r in rows])
+    am = np.array([r["adj_ms"] for r in rows])
+    ratio = am / pm
+    errs = [max(r["max_rel_err_theta"], r["rel_err_mu"]) for r in fd_rows]
+    errs_p = [max(r["polished_max_rel_err_theta"], r["polished_rel_err_mu"]) for r in fd_rows]
+    line = {
+        "metric": "adjoint/primal device time", "value": float(ratio.mean()), "unit": "x",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.profiles, "warmup": 1,
+        "ms_per_step": float((pm + am).mean()), "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 primal, f64 adjoint", "data": "synthetic: seeded inlet profiles 0.001 + N(0, 1e-4) m/s",
+        "config": {"workload": ADJ_WORKLOAD, "nx": nx, "ny": ny, "parameters": ny + 1,
+                   "objective": "mean p(first column) - mean p(last column)",
+                   "primal": "FP32, per-field criterion 1e-5 from rest", "adjoint_tol": 1e-8,
+                   "form": "single-launch adjoint solve (k_adjoint2d)"},
+        "primal_ms_mean": float(pm.mean()), "adjoint_ms_mean": float(am.mean()),
+        "ratio_max": float(ratio.max()),
+        "primal_iterations_mean": float(np.mean([r["primal_its"] for r in rows])),
+        "adjoint_iterations_mean": float(np.mean([r["adj_its"] for r in rows])),
+        "polish": {"outer_iterations": POLISH, "ms_mean": float(np.mean([r["polish_ms"] for r in rows]))},
+        "all_converged": bool(all(r["primal_converged"] and r["adj_converged"] for r in rows)),
+        "e2e": {"value": float(np.mean([r["wall_ms"] for r in rows])), "unit": "ms per gradient (host wall clock)",
+                "h2d_bytes_per_step": ny * 8, "d2h_bytes_per_step": (ny + 1) * 8},
+        "grad_vs_fd": {"profiles_checked": len(fd_rows), "parameters_each": ny + 1, "fd_step": "1e-3 relative",
+                       "fd_precision": "FP64", "fd_iters_from_base": args.fd_iters, "fd_seconds": t_fd,
+                       "max_rel_err": float(max(errs)) if errs else None,
+                       "max_rel_err_polished": float(max(errs_p)) if errs_p else None,
+                       "bound": 1e-4, "per_profile": fd_rows},
+        "gpu_launches": int(sum(r["launches"] for r in rows)),
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -337,6 +497,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.form == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

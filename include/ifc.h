@@ -179,6 +179,13 @@ typedef struct ifc_batch_result {
 int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result *results, void *const *fields_out,
                     double *device_ms);
 
+/* Replaces the west-inlet velocity profile of a handle created with an
+ * inlet_profile (ny*nz host doubles, stored in the handle's precision); the
+ * next solve, iteration or adjoint uses it.  IFC_BAD_ARGUMENT when the handle
+ * has no profile.  No counterpart in the reference (its inlet is a compiled-in
+ * constant); it lets a design loop update theta without rebuilding a handle. */
+int ifc_set_inlet_profile(ifc_solver *h, const double *profile);
+
 /* ---- differentiation form: discrete adjoint of the converged 2D solve ---- */
 /* Objectives of ifc_adjoint. */
 enum {

@@ -31,6 +31,7 @@ struct EngineBase {
     virtual int stats(ifc_stats *st) = 0;
     virtual int time_stage(int stage, int reps, double *ms, int *launches) = 0;
     virtual int adjoint(const AdjointReq &rq, ifc_adjoint_result *res) = 0;
+    virtual int set_inlet(const double *profile) = 0;
     std::string err;
 };
 
@@ -691,6 +692,20 @@ struct Engine : EngineBase {
             if (rc != IFC_OK) return rc;
             if (sq) sq[s] = ctl_h.last_sweep_sq[eq];
         }
+        return IFC_OK;
+    }
+
+    int set_inlet(const double *profile) override
+    {
+        if (!inlet_d || !profile) {
+            err = "set_inlet_profile: the handle was created without an inlet profile";
+            return IFC_BAD_ARGUMENT;
+        }
+        const size_t n = (size_t)P.g.ny * P.g.nz;
+        std::vector<T> h(n);
+        for (size_t q = 0; q < n; ++q) h[q] = (T)profile[q];
+        IFC_CK(cudaMemcpyAsync(inlet_d, h.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
+        IFC_CK(cudaStreamSynchronize(stream));
         return IFC_OK;
     }
 

@@ -217,6 +217,13 @@ int ifc_time_stage(ifc_solver *h, int stage, int reps, double *ms, int *launches
     IFC_END(h)
 }
 
+int ifc_set_inlet_profile(ifc_solver *h, const double *profile)
+{
+    IFC_GUARD(h)
+    return h->eng->set_inlet(profile);
+    IFC_END(h)
+}
+
 int ifc_adjoint(ifc_solver *h, int objective, const double *dJ_du, const double *dJ_dv, const double *dJ_dp,
                 int max_iter, double tol, double *dJ_dtheta, ifc_adjoint_result *result)
 {

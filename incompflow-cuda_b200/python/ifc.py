@@ -115,6 +115,7 @@ EXPORTS = {
     "ifc_adjoint": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, C.c_int, C.c_double, _DP,
                               C.POINTER(IfcAdjointResult)]),
     "ifc_adjoint_apply": (C.c_int, [C.c_void_p] + [_DP] * 12),
+    "ifc_set_inlet_profile": (C.c_int, [C.c_void_p, _DP]),
 }
 
 
@@ -331,6 +332,12 @@ class Solver:
 
     def write_vtk(self, path: str):
         self._check(load().ifc_write_vtk(self._h, path.encode()), "write_vtk")
+
+    def set_inlet_profile(self, profile):
+        a = np.ascontiguousarray(profile, dtype=np.float64)
+        if a.size != self.ny * self.nz:
+            raise ValueError(f"inlet profile has {a.size} values, expected {self.ny * self.nz}")
+        self._check(load().ifc_set_inlet_profile(self._h, _dptr(a)), "set_inlet_profile")
 
     def adjoint(self, objective: int = OBJ_PRESSURE_DROP, dJ_du=None, dJ_dv=None, dJ_dp=None,
                 max_iter: int = 200000, tol: float = 1e-10) -> tuple[np.ndarray, dict]:

@@ -184,3 +184,22 @@ def test_adjoint_is_deterministic_and_rejects_3d(gpu_ok):
     s3 = ifc.Solver(ifc.cavity3d(8))
     with pytest.raises(ifc.IfcError):
         s3.adjoint()
+
+
+def test_set_inlet_profile_matches_a_new_handle(gpu_ok):
+    cfg, theta = _channel(24, 10, precision="f", tol_u=1e-5, tol_v=1e-5, tol_p=1e-5)
+    s = ifc.Solver(cfg)
+    s.solve()
+    theta2 = theta * 1.1
+    s.set_inlet_profile(theta2)
+    s.set_uniform()
+    s.solve()
+    t = ifc.Solver(dict(cfg, inlet_profile=theta2))
+    t.solve()
+    for k in ("u", "v", "p"):
+        assert np.array_equal(s.get(k), t.get(k))
+    a, _ = s.adjoint(tol=1e-9)
+    b, _ = t.adjoint(tol=1e-9)
+    assert np.array_equal(a, b)
+    with pytest.raises(ifc.IfcError):
+        ifc.Solver(ifc.channel2d(24, 10)).set_inlet_profile(theta)
