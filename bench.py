@@ -53,13 +53,16 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--form", default="plain", choices=["plain", "adjoint"],
+    ap.add_argument("--form", default="plain", choices=["plain", "adjoint", "precision", "batch"],
                     help="plain: the headline throughput line; adjoint: the differentiation form")
     ap.add_argument("--profiles", type=int, default=32, help="adjoint form: seeded inlet profiles")
     ap.add_argument("--fd-profiles", type=int, default=1,
                     help="adjoint form: profiles whose 65 parameters are checked by central differences")
     ap.add_argument("--fd-iters", type=int, default=3000,
                     help="adjoint form: outer iterations of each warm-started FP64 finite-difference solve")
+    ap.add_argument("--n3d", type=int, default=128, help="precision form: cells per direction")
+    ap.add_argument("--max-outer", type=int, default=8000, help="precision form: outer-iteration cap")
+    ap.add_argument("--cases", type=int, default=256, help="batch form: cases")
     return ap.parse_args()
 
 
@@ -309,7 +312,7 @@ ADJ_WORKLOAD = "channel2d_256x64_adjoint"
 def adjoint_profile(k: int, ny: int = 64):
     import numpy as np
 
-    return 0.001 + np.random.default_rng(1000 + k).normal(0.0, 1e-4, ny)
+    return 0.001 + np.random.default_rng(k).normal(0.0, 1e-4, ny)
 
 
 def run_adjoint(args):
@@ -456,6 +459,143 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+PREC_WORKLOAD = "cavity3d_128_re400"
+
+
+def run_precision(args):
+    """Precision form: the 3D lid-driven cavity (128^3, Re 400, lid u=1 on the
+    top wall, solver settings of the 2D cavity: alpha 0.7/0.3, GS 5/5/5/50).
+    FP32 sweeps and assembly, FP64 norms, mass imbalance and p' pinning.
+      (a) FP32 from rest to convergence by the reference's own rule (every
+          relative norm over the running max of the pressure norm, 1e-5) --
+          the time to convergence;
+      (b) the same solver built in double, from rest, to the per-field rule
+          1e-5 (each norm over its own running max);
+      (c) the double build for exactly as many iterations as (a): the L2/Linf
+          error of (a)'s u, v, w, p (p modulo its mean) against it;
+    and the device time and compulsory bytes of each stage of one outer
+    iteration of the FP32 handle."""
+    import numpy as np
+    import torch
+
+    import ifc
+
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    n = args.n3d
+    cfg = ifc.cavity3d(n, re=400.0, numOuterIter=args.max_outer)
+    clocks = ClockSampler(local)
+    clocks.start()
+    s32 = ifc.Solver(dict(cfg, precision="f", criterion=ifc.CRIT_REFERENCE))
+    st32 = s32.solve()
+    k32 = st32["outer_iterations"]
+    s64 = ifc.Solver(dict(cfg, precision="d"))
+    st64 = s64.solve()
+    s64.close()
+    s64 = ifc.Solver(dict(cfg, precision="d"))
+    st64e = s64.iterate(k32)
+    clk = clocks.stop()
+
+    def fields(s):
+        f = {k: s.get(k).astype(np.float64) for k in ("u", "v", "w", "p")}
+        f["p"] -= f["p"].mean()
+        return f
+
+    a, b = fields(s32), fields(s64)
+    err = {k: {"rel_l2": float(np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k])),
+               "linf_rel": float(np.abs(a[k] - b[k]).max() / np.abs(b[k]).max())} for k in a}
+    N = n ** 3
+    nu, npc = cfg["nIter_u"], cfg["nIter_p"]
+    # compulsory unique bytes per launch sequence, FP32 (whole arrays; a half
+    # sweep reads whole cache lines of both colours)
+    byte_model = {
+        "mom_solve": (nu * 2 * (3 * 4 + 4 + 6 * 4)) * N,          # per half: faces, p, u/v/w read+write
+        "rhie_chow": (3 * 4 + 4 + 4 + 3 * 4 + 3 * 4 + 4) * N,     # u v w, p, aC in; faces, b_p out
+        "pcorr_solve": (4 + 4 + npc * 2 * (4 + 4 + 4 + 4)) * N,   # 1/aC once; per half 1/aC, p', b_p, p' write
+        "update": (4 + 4 + 4 * 3 + 3 * 4 + 4 + 3 * 4 * 2 + 4) * N,
+    }
+    peak, peak_kind = measured_peaks()
+    stages = {}
+    for name in ("mom_solve", "rhie_chow", "pcorr_solve", "update"):
+        ms_, nl = s32.time_stage(name, reps=5)
+        gbs = byte_model[name] / (ms_ * 1e-3) / 1e9
+        stages[name] = {"ms": ms_, "launches": nl, "compulsory_bytes": byte_model[name], "gbs": gbs,
+                        "frac_of_peak": gbs / peak}
+    line = {
+        "metric": "time to convergence", "value": st32["device_ms"] / 1e3, "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": st32["device_ms"], "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 sweeps, f64 reductions", "data": "synthetic: flow from rest",
+        "config": {"workload": PREC_WORKLOAD, "n": n, "criterion": "reference rule (norms over the p-norm max), 1e-5",
+                   "max_outer": args.max_outer},
+        "fp32": {"converged": bool(st32["converged"]), "outer_iterations": k32,
+                 "ms_per_outer_iteration": st32["device_ms"] / max(k32, 1),
+                 "cell_updates_per_s": st32["cell_updates"] / (st32["device_ms"] * 1e-3)},
+        "fp64_per_field": {"converged": bool(st64["converged"]), "outer_iterations": st64["outer_iterations"],
+                           "seconds": st64["device_ms"] / 1e3,
+                           "ms_per_outer_iteration": st64["device_ms"] / max(st64["outer_iterations"], 1)},
+        "error_vs_fp64_build_equal_iterations": err,
+        "stages_fp32": stages, "hbm_peak_gbs": peak, "peak_kind": peak_kind,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    s32.close()
+    s64.close()
+
+
+def run_batch(args):
+    """Batched form: --cases lid-driven cavities (nx, ny drawn from 32..256 in
+    steps of 32, Re log-uniform in [10, 1000], seed 0), each to the per-field
+    criterion 1e-5, in one persistent launch (ifc_batch_solve), against the
+    plain per-case loop (one handle per case, ifc_solve); solves/s of both and
+    the largest field difference between them."""
+    import numpy as np
+    import torch
+
+    import ifc
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    cases = ifc.batch_cases(args.cases, seed=0)
+    mine = ifc.shard_cases([c["nx"] * c["ny"] for c in cases], rank, world) if world > 1 else list(range(len(cases)))
+    sub = [cases[i] for i in mine]
+    # warm-up on a few small cases
+    ifc.batch_solve([ifc.cavity2d(32)] * 4, want_fields=False)
+    clocks = ClockSampler(local)
+    clocks.start()
+    res, fields, bms = ifc.batch_solve(sub)
+    clk = clocks.stop()
+    plain_ms, worst, nconv_b, nconv_p = 0.0, 0.0, 0, 0
+    for k, c in enumerate(sub):
+        s = ifc.Solver(c)
+        st = s.solve()
+        plain_ms += st["device_ms"]
+        nconv_p += int(st["converged"])
+        nconv_b += int(res[k]["converged"])
+        for f in ("u", "v"):
+            a = fields[k][f].astype(np.float64)
+            b = s.get(f).astype(np.float64)
+            worst = max(worst, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
+        s.close()
+    line = {
+        "metric": "converged solves/s", "value": len(sub) / (bms * 1e-3), "unit": "solves/s",
+        "higher_is_better": True, "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": bms,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded cavity cases from rest",
+        "config": {"workload": f"batch_cavity2d_{args.cases}", "cases_this_rank": len(sub),
+                   "sizes": "nx, ny in {32..256 step 32}", "re": "log-uniform [10, 1000]",
+                   "criterion": "per-field relative 1e-5"},
+        "plain_loop": {"solves_per_s": len(sub) / (plain_ms * 1e-3), "device_ms": plain_ms,
+                       "note": "sum of per-case ifc_solve device times, handle creation excluded"},
+        "speedup_vs_plain": plain_ms / bms,
+        "converged": {"batch": nconv_b, "plain": nconv_p, "of": len(sub)},
+        "max_rel_l2_batch_vs_plain_uv": worst,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -499,6 +639,10 @@ def main():
         run_reference(args)
     elif args.form == "adjoint":
         run_adjoint(args)
+    elif args.form == "precision":
+        run_precision(args)
+    elif args.form == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

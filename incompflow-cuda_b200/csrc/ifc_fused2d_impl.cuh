@@ -1,6 +1,8 @@
 // ifc_fused2d_impl.cuh -- host-side launch sequences of the fused 2D kernels.
 #pragma once
 
+#include <cstdlib>
+
 namespace ifc {
 
 // Tile shapes: FP32 tiles are 32 x 16 cells, FP64 tiles 32 x 8 (the staged
@@ -164,6 +166,8 @@ static int persist_kernel(Engine<T> &e, bool launch, int *capacity)
     pa.n_iter[2] = 0;
     pa.n_iter[3] = e.cfg.n_iter_p;
     pa.pin = e.pin ? 1 : 0;
+    const char *stall = std::getenv("IFC_TEST_STALL_BARRIER");
+    pa.stall_test = (stall && stall[0] == '1') ? 1 : 0;
     void *args[] = {&e.P, &e.f, &e.ctl, &e.partials, &e.barrier, &pa};
     return cudaLaunchCooperativeKernel((const void *)kern, dim3(tiles), dim3(S::NT), args, smem, e.stream) ==
                    cudaSuccess

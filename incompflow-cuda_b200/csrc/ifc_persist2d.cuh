@@ -158,6 +158,7 @@ struct LoopState {
 struct PersistArgs {
     int n_iter[4];
     int pin;
+    int stall_test;  // failure-detection test: CTA 0 leaves before its first barrier
 };
 
 // Inner early-exit bookkeeping for one equation after a pass (the rule of
@@ -235,6 +236,11 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 L.inner_max[q] = -1e20;
             }
         __syncthreads();
+
+        // Failure-detection test (IFC_TEST_STALL_BARRIER=1 in the environment):
+        // CTA 0 leaves without arriving, so every other CTA's bounded wait at the
+        // next barrier runs out and the launch ends with the timeout status.
+        if (pa.stall_test && blockIdx.x == 0) { failed = true; break; }
 
         // ---------------- momentum passes ----------------
         for (int pass = 0; pass < (npass_m > 0 ? npass_m : 1); ++pass) {
