@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -126,14 +127,15 @@ struct Engine : EngineBase {
     long long launches_per_iter = 0;  // kernels in one captured outer iteration
     long long last_launches = 0;
     AdjointCtx *adj = nullptr;        // discrete-adjoint buffers and graphs (first ifc_adjoint call)
+    bool pc3d = false;                // 3D p' solve as one cooperative launch (k_pc_solve3d)
+    PcBlocks pcb = {0, 0, 0, 0};
+    size_t pc3d_smem = 0;
+    static constexpr int kPcNT = 1024;
 
     ~Engine() override
     {
         adjoint_free(adj);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        if (body_exec) cudaGraphExecDestroy(body_exec);
-        if (body_graph) cudaGraphDestroy(body_graph);
+        destroy_graphs();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamSynchronize(stream);
@@ -215,9 +217,89 @@ struct Engine : EngineBase {
         if (c.sweeps_per_pass > 0) spp_mom = spp_p = spp_persist = c.sweeps_per_pass;
         if (fused && (rc = prepare_fused()) != IFC_OK) return rc;
         if ((rc = prepare_persist()) != IFC_OK) return rc;
+        if (dim == 3 && c.linear_solver == IFC_GAUSS_SEIDEL && (rc = prepare_pc3d()) != IFC_OK) return rc;
         if ((rc = set_uniform(0.0, 0.0, 0.0, 0.0, 273.0)) != IFC_OK) return rc;
-        if ((rc = build_graph()) != IFC_OK) return rc;
+        if ((rc = build_graph()) != IFC_OK && pc3d) {
+            // the cooperative p' launch could not be captured: per-half-sweep kernels
+            cudaGetLastError();
+            destroy_graphs();
+            pc3d = false;
+            rc = build_graph();
+        }
+        return rc;
+    }
+
+    void destroy_graphs()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (body_exec) cudaGraphExecDestroy(body_exec);
+        if (body_graph) cudaGraphDestroy(body_graph);
+        exec = nullptr;
+        graph = nullptr;
+        body_exec = nullptr;
+        body_graph = nullptr;
+        cond = 0;
+    }
+
+    // Row blocks of the single-launch 3D p' solve: the smallest blocks (fewest
+    // rows, then the shortest perimeter) whose count fits one CTA per SM and
+    // whose p' and b_p' fit the CTA's shared memory.
+    int prepare_pc3d()
+    {
+        pc3d = false;
+        const char *off = std::getenv("IFC_PC3D_OFF");
+        if (off && off[0] == '1') return IFC_OK;
+        int dev = 0, optin = 0, coop = 0;
+        IFC_CK(cudaGetDevice(&dev));
+        IFC_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        IFC_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        if (!coop) return IFC_OK;
+        const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
+        const size_t per_row = 2 * sizeof(T) * (size_t)nx;
+        const long long max_rows = ((long long)optin - 4096) / (long long)per_row;
+        if (max_rows < 1) return IFC_OK;
+        long long best = -1, best_per = 0;
+        PcBlocks b = {0, 0, 0, 0};
+        for (int bj = 1; bj <= ny; ++bj)
+            for (int bk = 1; bk <= nz && (long long)bj * bk <= max_rows; ++bk) {
+                const int nbj = (ny + bj - 1) / bj, nbk = (nz + bk - 1) / bk;
+                if ((long long)nbj * nbk > nsm) continue;
+                const long long rows = (long long)bj * bk, per = bj + bk;
+                if (best < 0 || rows < best || (rows == best && per < best_per)) {
+                    best = rows;
+                    best_per = per;
+                    b = {bj, bk, nbj, nbk};
+                }
+            }
+        if (best < 0) return IFC_OK;
+        const size_t smem = (size_t)b.bj * b.bk * per_row;
+        auto kern = k_pc_solve3d<T, kPcNT>;
+        IFC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        IFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPcNT, smem));
+        if (per_sm < 1 || (long long)per_sm * nsm < (long long)b.nbj * b.nbk) return IFC_OK;
+        pcb = b;
+        pc3d_smem = smem;
+        pc3d = true;
         return IFC_OK;
+    }
+
+    void enq_pc_solve3d()
+    {
+        cudaMemsetAsync(barrier, 0, sizeof(GridBarrier), stream);
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(pcb.nbj * pcb.nbk);
+        lc.blockDim = dim3(kPcNT);
+        lc.dynamicSmemBytes = pc3d_smem;
+        lc.stream = stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        cudaLaunchKernelEx(&lc, k_pc_solve3d<T, kPcNT>, P, f, ctl, partials, barrier, pcb, cfg.n_iter_p);
+        ++launches;
     }
 
     int set_uniform(double u, double v, double w, double p, double t) override
@@ -414,6 +496,11 @@ struct Engine : EngineBase {
     {
         if (DIM == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
             enq_fused_pcorr();
+        } else if (DIM == 3 && cfg.linear_solver == IFC_GAUSS_SEIDEL && pc3d) {
+            k_reset_inner_p<<<1, 1, 0, stream>>>(ctl);
+            k_recip_ac<T><<<grid(P.g.N), 256, 0, stream>>>(f.ac, f.rac, P.g.N);
+            launches += 2;
+            enq_pc_solve3d();
         } else if (DIM == 3 && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
             k_reset_inner_p<<<1, 1, 0, stream>>>(ctl);
             k_recip_ac<T><<<grid(P.g.N), 256, 0, stream>>>(f.ac, f.rac, P.g.N);

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "ifc_kernels.cuh"
+#include "ifc_persist2d.cuh"
 
 namespace ifc {
 
@@ -22,16 +23,6 @@ struct Half3D {
 };
 
 template <typename T>
-__device__ __forceinline__ void colored_ijk(long long q, int color, int hx, int ny, int &i, int &j, int &k)
-{
-    const int i2 = (int)(q % hx);
-    const int r = (int)(q / hx);
-    j = r % ny;
-    k = r / ny;
-    i = 2 * i2 + ((color + j + k) & 1);
-}
-
-template <typename T>
 __global__ void __launch_bounds__(256) k_mom_half3d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, Half3D h)
 {
     const Geo<T> &g = P.g;
@@ -40,33 +31,33 @@ __global__ void __launch_bounds__(256) k_mom_half3d(Params<T> P, Fields<T> f, Ct
     for (int c = 0; c < 3; ++c) act[c] = h.active[c] && !ctl->stop[c];
     if (!act[0] && !act[1] && !act[2] && !h.first) return;  // uniform
     const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
-    const int hx = (nx + 1) / 2;
-    const long long count = (long long)hx * ny * nz;
+    const int nrows = ny * nz, lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nwg = (int)((gridDim.x * blockDim.x) >> 5);
     T *phi[3] = {f.u, f.v, f.w};
     double sq[3] = {0.0, 0.0, 0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count;
-         q += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        colored_ijk<T>(q, h.color, hx, ny, i, j, k);
-        if (i >= nx) continue;
-        const int c = i + nx * (j + ny * k);
-        const int fu = i + (nx + 1) * (j + ny * k), fv = i + nx * (j + (ny + 1) * k);
-        T a[7], b[3];
-        mom_cell<T, 3>(P, i, j, k, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], f.wf[c], f.wf[c + pl], f.p[c],
-                       i > 0 ? f.p[c - 1] : (T)0, i < nx - 1 ? f.p[c + 1] : (T)0, j > 0 ? f.p[c - nx] : (T)0,
-                       j < ny - 1 ? f.p[c + nx] : (T)0, k > 0 ? f.p[c - pl] : (T)0, k < nz - 1 ? f.p[c + pl] : (T)0,
-                       a, b);
-        if (h.first) f.ac[c] = a[AC];
+    // one warp per x-row, lanes over the row's cells of this colour
+    for (int r = gw; r < nrows; r += nwg) {
+        const int j = r % ny, k = r / ny;
+        for (int i = ((h.color + j + k) & 1) + 2 * lane; i < nx; i += 64) {
+            const int c = i + nx * (j + ny * k);
+            const int fu = i + (nx + 1) * (j + ny * k), fv = i + nx * (j + (ny + 1) * k);
+            T a[7], b[3];
+            mom_cell<T, 3>(P, i, j, k, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], f.wf[c], f.wf[c + pl], f.p[c],
+                           i > 0 ? f.p[c - 1] : (T)0, i < nx - 1 ? f.p[c + 1] : (T)0, j > 0 ? f.p[c - nx] : (T)0,
+                           j < ny - 1 ? f.p[c + nx] : (T)0, k > 0 ? f.p[c - pl] : (T)0, k < nz - 1 ? f.p[c + pl] : (T)0,
+                           a, b);
+            if (h.first) f.ac[c] = a[AC];
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-            if (!act[m]) continue;
-            const T *o = phi[m];
-            const T pE = i != nx - 1 ? o[c + 1] : (T)0, pW = i != 0 ? o[c - 1] : (T)0;
-            const T pN = j != ny - 1 ? o[c + nx] : (T)0, pS = j != 0 ? o[c - nx] : (T)0;
-            const T pT = k != nz - 1 ? o[c + pl] : (T)0, pB = k != 0 ? o[c - pl] : (T)0;
-            T d;
-            phi[m][c] = point_update<T, 3>(a, b[m], o[c], pE, pW, pN, pS, pT, pB, g.relax[m], d);
-            sq[m] += (double)d * (double)d;
+            for (int m = 0; m < 3; ++m) {
+                if (!act[m]) continue;
+                const T *o = phi[m];
+                const T pE = i != nx - 1 ? o[c + 1] : (T)0, pW = i != 0 ? o[c - 1] : (T)0;
+                const T pN = j != ny - 1 ? o[c + nx] : (T)0, pS = j != 0 ? o[c - nx] : (T)0;
+                const T pT = k != nz - 1 ? o[c + pl] : (T)0, pB = k != 0 ? o[c - pl] : (T)0;
+                T d;
+                phi[m][c] = point_update<T, 3>(a, b[m], o[c], pE, pW, pN, pS, pT, pB, g.relax[m], d);
+                sq[m] += (double)d * (double)d;
+            }
         }
     }
     __shared__ double tot[3];
@@ -97,38 +88,38 @@ __global__ void __launch_bounds__(256) k_pc_half3d(Params<T> P, Fields<T> f, con
     const Geo<T> &g = P.g;
     if (ctl->stop[EQ_P]) return;  // uniform
     const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
-    const int hx = (nx + 1) / 2;
-    const long long count = (long long)hx * ny * nz;
+    const int nrows = ny * nz, lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nwg = (int)((gridDim.x * blockDim.x) >> 5);
     double sq[1] = {0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count;
-         q += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        colored_ijk<T>(q, color, hx, ny, i, j, k);
-        if (i >= nx) continue;
-        const int c = i + nx * (j + ny * k);
-        const T r = rac[c];
-        T a[7];
-        a[AE] = i < nx - 1 ? (T)(P.d.Kx * (double)(T)(r + rac[c + 1])) : (T)0;
-        a[AW] = i > 0 ? (T)(P.d.Kx * (double)(T)(r + rac[c - 1])) : (T)0;
-        a[AN] = j < ny - 1 ? (T)(P.d.Ky * (double)(T)(r + rac[c + nx])) : (T)0;
-        a[AS] = j > 0 ? (T)(P.d.Ky * (double)(T)(r + rac[c - nx])) : (T)0;
-        a[AT] = k < nz - 1 ? (T)(P.d.Kz * (double)(T)(r + rac[c + pl])) : (T)0;
-        a[AB] = k > 0 ? (T)(P.d.Kz * (double)(T)(r + rac[c - pl])) : (T)0;
-        a[AC] = -(a[AE] + a[AW] + a[AN] + a[AS]);
-        a[AC] += -(a[AT] + a[AB]);
-        const T *o = f.pc;
-        // The solve starts from p' = 0 (src/Solver.cu:193) without clearing the
-        // array: in the first red half every value is 0 (zero_mode 1); in the
-        // first black half the neighbours are the red cells just written and
-        // only the cell itself is still 0 (zero_mode 2).
-        const bool zn = zero_mode == 1;
-        const T pE = (!zn && i != nx - 1) ? o[c + 1] : (T)0, pW = (!zn && i != 0) ? o[c - 1] : (T)0;
-        const T pN = (!zn && j != ny - 1) ? o[c + nx] : (T)0, pS = (!zn && j != 0) ? o[c - nx] : (T)0;
-        const T pT = (!zn && k != nz - 1) ? o[c + pl] : (T)0, pB = (!zn && k != 0) ? o[c - pl] : (T)0;
-        const T pc = zero_mode ? (T)0 : o[c];
-        T d;
-        f.pc[c] = point_update<T, 3>(a, f.sp[c], pc, pE, pW, pN, pS, pT, pB, g.relax[EQ_P], d);
-        sq[0] += (double)d * (double)d;
+    // one warp per x-row, lanes over the row's cells of this colour
+    for (int r = gw; r < nrows; r += nwg) {
+        const int j = r % ny, k = r / ny;
+        for (int i = ((color + j + k) & 1) + 2 * lane; i < nx; i += 64) {
+            const int c = i + nx * (j + ny * k);
+            const T rr = rac[c];
+            T a[7];
+            a[AE] = i < nx - 1 ? (T)(P.d.Kx * (double)(T)(rr + rac[c + 1])) : (T)0;
+            a[AW] = i > 0 ? (T)(P.d.Kx * (double)(T)(rr + rac[c - 1])) : (T)0;
+            a[AN] = j < ny - 1 ? (T)(P.d.Ky * (double)(T)(rr + rac[c + nx])) : (T)0;
+            a[AS] = j > 0 ? (T)(P.d.Ky * (double)(T)(rr + rac[c - nx])) : (T)0;
+            a[AT] = k < nz - 1 ? (T)(P.d.Kz * (double)(T)(rr + rac[c + pl])) : (T)0;
+            a[AB] = k > 0 ? (T)(P.d.Kz * (double)(T)(rr + rac[c - pl])) : (T)0;
+            a[AC] = -(a[AE] + a[AW] + a[AN] + a[AS]);
+            a[AC] += -(a[AT] + a[AB]);
+            const T *o = f.pc;
+            // The solve starts from p' = 0 (src/Solver.cu:193) without clearing the
+            // array: in the first red half every value is 0 (zero_mode 1); in the
+            // first black half the neighbours are the red cells just written and
+            // only the cell itself is still 0 (zero_mode 2).
+            const bool zn = zero_mode == 1;
+            const T pE = (!zn && i != nx - 1) ? o[c + 1] : (T)0, pW = (!zn && i != 0) ? o[c - 1] : (T)0;
+            const T pN = (!zn && j != ny - 1) ? o[c + nx] : (T)0, pS = (!zn && j != 0) ? o[c - nx] : (T)0;
+            const T pT = (!zn && k != nz - 1) ? o[c + pl] : (T)0, pB = (!zn && k != 0) ? o[c - pl] : (T)0;
+            const T pc = zero_mode ? (T)0 : o[c];
+            T d;
+            f.pc[c] = point_update<T, 3>(a, f.sp[c], pc, pE, pW, pN, pS, pT, pB, g.relax[EQ_P], d);
+            sq[0] += (double)d * (double)d;
+        }
     }
     __shared__ double tot[1];
     if (grid_reduce<1>(sq, partials, ctl, tot) && threadIdx.x == 0) {
@@ -139,6 +130,164 @@ __global__ void __launch_bounds__(256) k_pc_half3d(Params<T> P, Fields<T> f, con
             finish_sweeps(ctl, EQ_P, &s, 1, N, g.tol[EQ_P]);
         }
     }
+}
+
+// ---- the whole 3D p' solve in one cooperative launch -----------------------
+// Each CTA owns a rectangular block of x-rows (all i, j in [j0, j0+bj), k in
+// [k0, k0+bk)) and keeps p' and b_p' of its cells in shared memory for every
+// sweep of the solve.  The p' links do not change during the solve, so each
+// CTA first builds them for its cells (kernels.cuh:518-537, the same FP64
+// products as k_pc_half3d) into the coefficient planes aC, aE, aN, aT; a
+// cell's west, south and bottom links are its neighbours' east, north and top
+// links.  A half sweep then updates the CTA's cells of one colour; p'
+// neighbours in rows owned by another CTA come from global memory, where every
+// CTA publishes the cells of its boundary rows after each half sweep; a
+// bounded grid barrier separates the half sweeps.  The per-sweep FP64 sums are
+// reduced in a fixed order by every CTA, so each takes the same inner
+// early-exit decision (src/Solver.cu:955-962).  Per cell the arithmetic is
+// k_pc_half3d's, so the result is bit-identical to the per-half-sweep kernels.
+struct PcBlocks {
+    int bj, bk;    // rows per block along j and k
+    int nbj, nbk;  // blocks along j and k
+};
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_pc_solve3d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials,
+                                                      GridBarrier *bar, PcBlocks B, int n_sweeps)
+{
+    const Geo<T> &g = P.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
+    const int G = gridDim.x, tid = threadIdx.x;
+    const int j0 = (blockIdx.x % B.nbj) * B.bj, k0 = (blockIdx.x / B.nbj) * B.bk;
+    const int nj = min(B.bj, ny - j0), nk = min(B.bk, nz - k0);
+    const int cap = nx * B.bj * B.bk;
+    const int nrow = nj * nk;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int ln = nx, lt = nx * nj;  // local strides to the next row in j and in k
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *s_pc = reinterpret_cast<T *>(smem_raw);
+    T *s_sp = s_pc + cap;
+    T *cC = f.pcoef + (size_t)N * AC, *cE = f.pcoef + (size_t)N * AE;
+    T *cN = f.pcoef + (size_t)N * AN, *cT = f.pcoef + (size_t)N * AT;
+    __shared__ double red[NT / 32];
+    __shared__ double tot2[2];
+
+    // links of the CTA's cells, b_p', p' = 0
+    for (int r = warp; r < nrow; r += NT / 32) {
+        const int j = j0 + r % nj, k = k0 + r / nj;
+        const int lrow = nx * r, crow = nx * (j + ny * k);
+        for (int i = lane; i < nx; i += 32) {
+            const int c = crow + i;
+            const T rr = f.rac[c];
+            T a[7];
+            a[AE] = i < nx - 1 ? (T)(P.d.Kx * (double)(T)(rr + f.rac[c + 1])) : (T)0;
+            a[AW] = i > 0 ? (T)(P.d.Kx * (double)(T)(rr + f.rac[c - 1])) : (T)0;
+            a[AN] = j < ny - 1 ? (T)(P.d.Ky * (double)(T)(rr + f.rac[c + nx])) : (T)0;
+            a[AS] = j > 0 ? (T)(P.d.Ky * (double)(T)(rr + f.rac[c - nx])) : (T)0;
+            a[AT] = k < nz - 1 ? (T)(P.d.Kz * (double)(T)(rr + f.rac[c + pl])) : (T)0;
+            a[AB] = k > 0 ? (T)(P.d.Kz * (double)(T)(rr + f.rac[c - pl])) : (T)0;
+            a[AC] = -(a[AE] + a[AW] + a[AN] + a[AS]);
+            a[AC] += -(a[AT] + a[AB]);
+            cC[c] = a[AC];
+            cE[c] = a[AE];
+            cN[c] = a[AN];
+            cT[c] = a[AT];
+            s_sp[lrow + i] = f.sp[c];
+            s_pc[lrow + i] = (T)0;
+        }
+    }
+    double mx = ctl->inner_max[EQ_P];
+    int sw = ctl->sweeps[EQ_P];
+    bool stop = ctl->stop[EQ_P] != 0;
+    double last_sq = 0.0;
+    unsigned int epoch = 0;
+    bool failed = !grid_sync(bar, G, epoch);
+
+    for (int s = 0; s < n_sweeps && !stop && !failed; ++s) {
+        for (int color = 0; color < 2; ++color) {
+            const int zero_mode = s == 0 ? (color == 0 ? 1 : 2) : 0;
+            const bool zn = zero_mode == 1;
+            double sq = 0.0;
+            // one warp per row of the block (row r = jj + nj*kk), lanes along x
+            for (int r = warp; r < nrow; r += NT / 32) {
+                const int jj = r % nj, kk = r / nj;
+                const int j = j0 + jj, k = k0 + kk;
+                const int lrow = nx * r, crow = nx * (j + ny * k);
+                const bool inN = jj + 1 < nj, inS = jj > 0, inT = kk + 1 < nk, inB = kk > 0;
+                for (int i = ((color + j + k) & 1) + 2 * lane; i < nx; i += 64) {
+                    const int l = lrow + i, c = crow + i;
+                    T a[7];
+                    a[AC] = cC[c];
+                    a[AE] = cE[c];
+                    a[AW] = i > 0 ? cE[c - 1] : (T)0;
+                    a[AN] = cN[c];
+                    a[AS] = j > 0 ? cN[c - nx] : (T)0;
+                    a[AT] = cT[c];
+                    a[AB] = k > 0 ? cT[c - pl] : (T)0;
+                    const T pE = (!zn && i != nx - 1) ? s_pc[l + 1] : (T)0;
+                    const T pW = (!zn && i != 0) ? s_pc[l - 1] : (T)0;
+                    const T pN = (!zn && j != ny - 1) ? (inN ? s_pc[l + ln] : __ldcg(&f.pc[c + nx])) : (T)0;
+                    const T pS = (!zn && j != 0) ? (inS ? s_pc[l - ln] : __ldcg(&f.pc[c - nx])) : (T)0;
+                    const T pT = (!zn && k != nz - 1) ? (inT ? s_pc[l + lt] : __ldcg(&f.pc[c + pl])) : (T)0;
+                    const T pB = (!zn && k != 0) ? (inB ? s_pc[l - lt] : __ldcg(&f.pc[c - pl])) : (T)0;
+                    const T pc = zero_mode ? (T)0 : s_pc[l];
+                    T d;
+                    s_pc[l] = point_update<T, 3>(a, s_sp[l], pc, pE, pW, pN, pS, pT, pB, g.relax[EQ_P], d);
+                    sq += (double)d * (double)d;
+                }
+            }
+            __syncthreads();
+            // publish this colour's cells of the boundary rows
+            for (int r = warp; r < nrow; r += NT / 32) {
+                const int jj = r % nj, kk = r / nj;
+                if (jj != 0 && jj != nj - 1 && kk != 0 && kk != nk - 1) continue;
+                const int j = j0 + jj, k = k0 + kk;
+                const int lrow = nx * r, crow = nx * (j + ny * k);
+                for (int i = ((color + j + k) & 1) + 2 * lane; i < nx; i += 64) f.pc[crow + i] = s_pc[lrow + i];
+            }
+            // this CTA's sum of the half sweep, in warp order
+            sq = warp_sum(sq);
+            if (lane == 0) red[warp] = sq;
+            __syncthreads();
+            if (tid == 0) {
+                double x = 0.0;
+                for (int w = 0; w < NT / 32; ++w) x += red[w];
+                partials[(size_t)(2 * (s & 1) + color) * G + blockIdx.x] = x;
+            }
+            if (!grid_sync(bar, G, epoch)) { failed = true; break; }
+        }
+        if (failed) break;
+        // grid sums of both halves, fixed order, identical in every CTA
+        if (tid < 64) {
+            const int color = tid >> 5;
+            double x = 0.0;
+            for (int b = lane; b < G; b += 32) x += __ldcg(&partials[(size_t)(2 * (s & 1) + color) * G + b]);
+            x = warp_sum(x);
+            if (lane == 0) tot2[color] = x;
+        }
+        __syncthreads();
+        const double ssq = tot2[0] + tot2[1];
+        const double rms = sqrt(ssq / (double)N);
+        if (rms > mx) mx = rms;
+        if (rms / (mx + 1e-20) < g.tol[EQ_P]) stop = true;
+        ++sw;
+        last_sq = ssq;
+        __syncthreads();  // tot2 is rewritten only after the next sweep's barriers
+    }
+    for (int r = warp; r < nrow; r += NT / 32) {
+        const int j = j0 + r % nj, k = k0 + r / nj;
+        const int lrow = nx * r, crow = nx * (j + ny * k);
+        for (int i = lane; i < nx; i += 32) f.pc[crow + i] = s_pc[lrow + i];
+    }
+    if (blockIdx.x == 0 && tid == 0 && !failed) {
+        const int done = sw - ctl->sweeps[EQ_P];
+        ctl->cell_updates += (long long)done * N;
+        ctl->inner_max[EQ_P] = mx;
+        ctl->sweeps[EQ_P] = sw;
+        if (done > 0) ctl->last_sweep_sq[EQ_P] = last_sq;
+        if (stop) ctl->stop[EQ_P] = 1;
+    }
+    if (tid == 0 && (failed || bar->err)) atomicExch(&ctl->status, 3);
 }
 
 }  // namespace ifc

@@ -372,6 +372,7 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
     const double mass_sq = ctl->sq[SQ_MASS];
     const int it0 = ctl->it, it_begin = ctl->it_begin, it_stop = ctl->it_stop, act = ctl->act;
     const int log_level = ctl->log_level, log_n = ctl->log_n;
+    const int status0 = ctl->status;  // 3: a bounded wait of this iteration gave up
     double maxn[8];
     int sweeps[4];
 #pragma unroll
@@ -422,7 +423,7 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
     if (d3) conv = conv && rel[3] < g.tol[EQ_W] && rel[6] < g.tol[EQ_W];
     conv = conv || n[7] < g.tol_mass;
     const int local = it - it_begin;
-    const bool last = it >= it_stop || (act && conv) || bad;
+    const bool last = it >= it_stop || (act && conv) || bad || status0 == 3;
 
 #pragma unroll
     for (int q = 0; q < 7; ++q) ctl->sq[q] = tot[q];
