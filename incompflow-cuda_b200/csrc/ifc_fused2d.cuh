@@ -102,7 +102,8 @@ __device__ __forceinline__ int tile_distance(int q)
 
 // ---- momentum: assembly + KS red-black sweeps of u and v -------------------
 template <typename T, int TX, int TY, int KS, int NT>
-__global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, PassArgs pa)
+__global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, PassArgs pa,
+                                                   const T *u_in, const T *v_in, T *u_out, T *v_out)
 {
     constexpr int H = 2 * KS;
     using R = Region<TX, TY, H>;
@@ -112,7 +113,6 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
     bool act[2];
     act[0] = pa.ns[0] > 0 && !ctl->stop[EQ_U];
     act[1] = pa.ns[1] > 0 && !ctl->stop[EQ_V];
-    if (!act[0] && !act[1] && !pa.first) return;  // same in every block
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *su = reinterpret_cast<T *>(smem_raw);
@@ -130,8 +130,8 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
         const int gi = gx0 + a, gj = gy0 + b;
         const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
         const int id = gi + nx * gj;
-        su[q] = in ? f.u[id] : (T)0;
-        sv[q] = in ? f.v[id] : (T)0;
+        su[q] = in ? u_in[id] : (T)0;
+        sv[q] = in ? v_in[id] : (T)0;
         sp[q] = in ? f.p[id] : (T)0;
     }
     int cq[2][CPT];
@@ -215,8 +215,8 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
         const int gi = gx0 + a, gj = gy0 + b;
         if (gi >= nx || gj >= ny) continue;
         const int id = gi + nx * gj;
-        if (act[0]) f.u[id] = su[b * W + a];
-        if (act[1]) f.v[id] = sv[b * W + a];
+        u_out[id] = su[b * W + a];
+        v_out[id] = sv[b * W + a];
     }
 
     double flat[2 * KS];
@@ -233,14 +233,15 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
 
 // ---- pressure correction: KS red-black sweeps ------------------------------
 template <typename T, int TX, int TY, int KS, int NT>
-__global__ void __launch_bounds__(NT) k_pc_pass2d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, PassArgs pa)
+__global__ void __launch_bounds__(NT) k_pc_pass2d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, PassArgs pa,
+                                                  const T *pc_in, T *pc_out)
 {
     constexpr int H = 2 * KS;
     using R = Region<TX, TY, H>;
     constexpr int W = R::W, NR = R::NR;
     constexpr int CPT = (R::NHALF + NT - 1) / NT;
     const Geo<T> &g = P.g;
-    if (pa.ns[0] <= 0 || ctl->stop[EQ_P]) return;  // same in every block
+    const bool active = pa.ns[0] > 0 && !ctl->stop[EQ_P];  // same in every block
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sx = reinterpret_cast<T *>(smem_raw);  // p'
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(NT) k_pc_pass2d(Params<T> P, Fields<T> f, Ctl 
         const int gi = gx0 + a, gj = gy0 + b;
         const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
         const int id = gi + nx * gj;
-        sx[q] = (in && !pa.first) ? f.pc[id] : (T)0;
+        sx[q] = (in && !pa.first) ? pc_in[id] : (T)0;
         sr[q] = in ? (T)1 / f.ac[id] : (T)0;
     }
     int cq[2][CPT];
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(NT) k_pc_pass2d(Params<T> P, Fields<T> f, Ctl 
         for (int k = 0; k < CPT; ++k) dq[c][k] = tile_distance<W, H, TX, TY>(cq[c][k]);
 #pragma unroll
     for (int s = 0; s < KS; ++s) {
-        if (s >= pa.ns[0]) break;
+        if (!active || s >= pa.ns[0]) break;
 #pragma unroll
         for (int color = 0; color < 2; ++color) {
             const int reach = 2 * pa.ns[0] - 1 - (2 * s + color);
@@ -326,8 +327,9 @@ __global__ void __launch_bounds__(NT) k_pc_pass2d(Params<T> P, Fields<T> f, Ctl 
         const int a = H + q % TX, b = H + q / TX;
         const int gi = gx0 + a, gj = gy0 + b;
         if (gi >= nx || gj >= ny) continue;
-        f.pc[gi + nx * gj] = sx[b * W + a];
+        pc_out[gi + nx * gj] = sx[b * W + a];
     }
+    if (!active) return;  // uniform: the copy above keeps the output buffer current
 
     __shared__ double tot[KS];
     if (grid_reduce<KS>(acc, partials, ctl, tot) && tid == 0) finish_sweeps(ctl, EQ_P, tot, pa.ns[0], g.N, g.tol[EQ_P]);

@@ -5,6 +5,13 @@
 
 namespace ifc {
 
+// Source and destination buffers of one fused pass (u, v or p').
+template <typename T>
+struct PassBufs {
+    const T *in[2];
+    T *out[2];
+};
+
 // Tile shapes: FP32 tiles are 32 x 16 cells, FP64 tiles 32 x 8 (the staged
 // region of an FP64 tile needs twice the shared memory per cell).
 template <typename T>
@@ -13,7 +20,7 @@ struct TileShape2D {
 };
 
 template <typename T, int KS>
-static int launch_mom_pass(Engine<T> &e, const PassArgs &pa, bool prepare = false)
+static int launch_mom_pass(Engine<T> &e, const PassArgs &pa, const PassBufs<T> &b, bool prepare = false)
 {
     using S = TileShape2D<T>;
     using R = Region<S::TX, S::TY, 2 * KS>;
@@ -22,13 +29,13 @@ static int launch_mom_pass(Engine<T> &e, const PassArgs &pa, bool prepare = fals
     if (prepare) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
                                cudaSuccess ? IFC_OK : IFC_CUDA_ERROR;
     const int tiles = ((e.P.g.nx + S::TX - 1) / S::TX) * ((e.P.g.ny + S::TY - 1) / S::TY);
-    kern<<<tiles, S::NT, smem, e.stream>>>(e.P, e.f, e.ctl, e.partials, pa);
+    kern<<<tiles, S::NT, smem, e.stream>>>(e.P, e.f, e.ctl, e.partials, pa, b.in[0], b.in[1], b.out[0], b.out[1]);
     ++e.launches;
     return IFC_OK;
 }
 
 template <typename T, int KS>
-static int launch_pc_pass(Engine<T> &e, const PassArgs &pa, bool prepare = false)
+static int launch_pc_pass(Engine<T> &e, const PassArgs &pa, const PassBufs<T> &b, bool prepare = false)
 {
     using S = TileShape2D<T>;
     using R = Region<S::TX, S::TY, 2 * KS>;
@@ -37,7 +44,7 @@ static int launch_pc_pass(Engine<T> &e, const PassArgs &pa, bool prepare = false
     if (prepare) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
                                cudaSuccess ? IFC_OK : IFC_CUDA_ERROR;
     const int tiles = ((e.P.g.nx + S::TX - 1) / S::TX) * ((e.P.g.ny + S::TY - 1) / S::TY);
-    kern<<<tiles, S::NT, smem, e.stream>>>(e.P, e.f, e.ctl, e.partials, pa);
+    kern<<<tiles, S::NT, smem, e.stream>>>(e.P, e.f, e.ctl, e.partials, pa, b.in[0], b.out[0]);
     ++e.launches;
     return IFC_OK;
 }
@@ -54,30 +61,30 @@ static inline int fused_ks(int want)
 }
 
 template <typename T>
-static int dispatch_mom(Engine<T> &e, int ks, const PassArgs &pa, bool prepare = false)
+static int dispatch_mom(Engine<T> &e, int ks, const PassArgs &pa, const PassBufs<T> &b, bool prepare = false)
 {
     switch (ks) {
-    case 1: return launch_mom_pass<T, 1>(e, pa, prepare);
-    case 2: return launch_mom_pass<T, 2>(e, pa, prepare);
-    case 3: return launch_mom_pass<T, 3>(e, pa, prepare);
-    case 4: return launch_mom_pass<T, 4>(e, pa, prepare);
-    case 5: return launch_mom_pass<T, 5>(e, pa, prepare);
-    case 6: return launch_mom_pass<T, 6>(e, pa, prepare);
-    default: return launch_mom_pass<T, 8>(e, pa, prepare);
+    case 1: return launch_mom_pass<T, 1>(e, pa, b, prepare);
+    case 2: return launch_mom_pass<T, 2>(e, pa, b, prepare);
+    case 3: return launch_mom_pass<T, 3>(e, pa, b, prepare);
+    case 4: return launch_mom_pass<T, 4>(e, pa, b, prepare);
+    case 5: return launch_mom_pass<T, 5>(e, pa, b, prepare);
+    case 6: return launch_mom_pass<T, 6>(e, pa, b, prepare);
+    default: return launch_mom_pass<T, 8>(e, pa, b, prepare);
     }
 }
 
 template <typename T>
-static int dispatch_pc(Engine<T> &e, int ks, const PassArgs &pa, bool prepare = false)
+static int dispatch_pc(Engine<T> &e, int ks, const PassArgs &pa, const PassBufs<T> &b, bool prepare = false)
 {
     switch (ks) {
-    case 1: return launch_pc_pass<T, 1>(e, pa, prepare);
-    case 2: return launch_pc_pass<T, 2>(e, pa, prepare);
-    case 3: return launch_pc_pass<T, 3>(e, pa, prepare);
-    case 4: return launch_pc_pass<T, 4>(e, pa, prepare);
-    case 5: return launch_pc_pass<T, 5>(e, pa, prepare);
-    case 6: return launch_pc_pass<T, 6>(e, pa, prepare);
-    default: return launch_pc_pass<T, 8>(e, pa, prepare);
+    case 1: return launch_pc_pass<T, 1>(e, pa, b, prepare);
+    case 2: return launch_pc_pass<T, 2>(e, pa, b, prepare);
+    case 3: return launch_pc_pass<T, 3>(e, pa, b, prepare);
+    case 4: return launch_pc_pass<T, 4>(e, pa, b, prepare);
+    case 5: return launch_pc_pass<T, 5>(e, pa, b, prepare);
+    case 6: return launch_pc_pass<T, 6>(e, pa, b, prepare);
+    default: return launch_pc_pass<T, 8>(e, pa, b, prepare);
     }
 }
 
@@ -88,8 +95,9 @@ template <typename T>
 int Engine<T>::prepare_fused()
 {
     PassArgs pa = {};
-    int rc = dispatch_mom<T>(*this, fused_ks(spp_mom), pa, true);
-    if (rc == IFC_OK) rc = dispatch_pc<T>(*this, fused_ks(spp_p), pa, true);
+    PassBufs<T> b = {};
+    int rc = dispatch_mom<T>(*this, fused_ks(spp_mom), pa, b, true);
+    if (rc == IFC_OK) rc = dispatch_pc<T>(*this, fused_ks(spp_p), pa, b, true);
     if (rc != IFC_OK) err = "cudaFuncSetAttribute(MaxDynamicSharedMemorySize) failed";
     return rc;
 }
@@ -102,13 +110,22 @@ void Engine<T>::enq_fused_mom()
     const int nmax = nu > nv ? nu : nv;
     int npass = (nmax + ks - 1) / ks;
     if (npass < 1) npass = 1;  // the first pass also stores aC
+    // A pass stages halos from one buffer and writes its tiles to the other,
+    // so no tile reads a neighbour tile's values of the same pass.
+    const size_t N = (size_t)P.g.N;
+    T *bu[2] = {f.u, f.tmp}, *bv[2] = {f.v, f.tmp + N};
     for (int pass = 0; pass < npass; ++pass) {
         PassArgs pa;
         pa.ns[0] = clamp_sweeps(nu, pass, ks);
         pa.ns[1] = clamp_sweeps(nv, pass, ks);
         pa.ns[2] = 0;
         pa.first = pass == 0;
-        dispatch_mom<T>(*this, ks, pa);
+        PassBufs<T> b = {{bu[pass & 1], bv[pass & 1]}, {bu[(pass + 1) & 1], bv[(pass + 1) & 1]}};
+        dispatch_mom<T>(*this, ks, pa, b);
+    }
+    if (npass & 1) {
+        cudaMemcpyAsync(f.u, f.tmp, N * sizeof(T), cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(f.v, f.tmp + N, N * sizeof(T), cudaMemcpyDeviceToDevice, stream);
     }
 }
 
@@ -122,12 +139,16 @@ void Engine<T>::enq_fused_pcorr()
         return;
     }
     const int npass = (np + ks - 1) / ks;
+    // Ping-pong as for the momentum passes, ordered so that the last pass
+    // writes f.pc (the first pass reads nothing: p' starts from 0).
+    T *bp[2] = {f.pc, f.tmp + 2 * (size_t)P.g.N};
     for (int pass = 0; pass < npass; ++pass) {
         PassArgs pa;
         pa.ns[0] = clamp_sweeps(np, pass, ks);
         pa.ns[1] = pa.ns[2] = 0;
         pa.first = pass == 0;
-        dispatch_pc<T>(*this, ks, pa);
+        PassBufs<T> b = {{bp[(npass - pass) & 1], nullptr}, {bp[(npass - 1 - pass) & 1], nullptr}};
+        dispatch_pc<T>(*this, ks, pa, b);
     }
 }
 

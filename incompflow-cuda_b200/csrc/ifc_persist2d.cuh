@@ -227,8 +227,13 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
     const int npass_p = (pa.n_iter[3] + KS - 1) / KS;
     bool failed = false;
     unsigned int epoch = 0;
+    // A pass stages halos from one buffer and writes its tile to the other, so
+    // no tile reads a neighbour tile's values of the same pass; `mcur`/`pcur`
+    // (the same in every CTA) say which buffer holds the current u, v / p'.
+    T *bu[2] = {f.u, f.tmp}, *bv[2] = {f.v, f.tmp + N}, *bp[2] = {f.pc, f.tmp + 2 * (size_t)N};
 
     while (!L.done) {
+        int mcur = 0, pcur = 0;
         if (tid == 0)
             for (int q = 0; q < 4; ++q) {
                 L.stop[q] = 0;
@@ -253,8 +258,8 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 const int gi = gx0 + a, gj = gy0 + b;
                 const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
                 const int id = gi + nx * gj;
-                s0[q] = in ? f.u[id] : (T)0;
-                s1[q] = in ? f.v[id] : (T)0;
+                s0[q] = in ? bu[mcur][id] : (T)0;
+                s1[q] = in ? bv[mcur][id] : (T)0;
                 s2[q] = in ? f.p[id] : (T)0;
             }
             __syncthreads();
@@ -332,9 +337,10 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 const int gi = gx0 + a, gj = gy0 + b;
                 if (gi >= nx || gj >= ny) continue;
                 const int id = gi + nx * gj;
-                if (au) f.u[id] = s0[b * W + a];
-                if (av) f.v[id] = s1[b * W + a];
+                bu[mcur ^ 1][id] = s0[b * W + a];
+                bv[mcur ^ 1][id] = s1[b * W + a];
             }
+            mcur ^= 1;
             block_partials<2 * KS, 2 * KS, NT>(&wred[0][0], partials, G);
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
             reduce_partials<2 * KS, NT>(partials, G, tot);
@@ -347,16 +353,19 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         if (failed) break;
 
         // ------------- Rhie-Chow faces, face BCs, p' source -------------
+        Fields<T> fc = f;  // the current u, v
+        fc.u = bu[mcur];
+        fc.v = bv[mcur];
         {
             double m[1] = {0.0};
             for (int q = tid; q < TX * TY; q += NT) {
                 const int i = x0 + q % TX, j = y0 + q / TX;
                 if (i >= nx || j >= ny) continue;
                 const int c = i + nx * j;
-                const T uw = i == 0 ? face_bc(g, WEST, 0, f.u[c], j) : rc_x(P, f, i, j);
-                const T ue = i == nx - 1 ? face_bc(g, EAST, 0, f.u[c], j) : rc_x(P, f, i + 1, j);
-                const T vs = j == 0 ? face_bc(g, SOUTH, 1, f.v[c], 0) : rc_y(P, f, i, j);
-                const T vn = j == ny - 1 ? face_bc(g, NORTH, 1, f.v[c], 0) : rc_y(P, f, i, j + 1);
+                const T uw = i == 0 ? face_bc(g, WEST, 0, fc.u[c], j) : rc_x(P, fc, i, j);
+                const T ue = i == nx - 1 ? face_bc(g, EAST, 0, fc.u[c], j) : rc_x(P, fc, i + 1, j);
+                const T vs = j == 0 ? face_bc(g, SOUTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j);
+                const T vn = j == ny - 1 ? face_bc(g, NORTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j + 1);
                 const T b = mass_imbalance<T, 2>(g, uw, ue, vs, vn, (T)0, (T)0);
                 f.uf[i + (nx + 1) * j] = uw;
                 if (i == nx - 1) f.uf[nx + (nx + 1) * j] = ue;
@@ -378,7 +387,7 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 const int gi = gx0 + a, gj = gy0 + b;
                 const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
                 const int id = gi + nx * gj;
-                s0[q] = (in && pass > 0) ? f.pc[id] : (T)0;
+                s0[q] = (in && pass > 0) ? bp[pcur][id] : (T)0;
                 s1[q] = in ? (T)1 / f.ac[id] : (T)0;
             }
             __syncthreads();
@@ -435,8 +444,9 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 const int a = H + q % TX, b = H + q / TX;
                 const int gi = gx0 + a, gj = gy0 + b;
                 if (gi >= nx || gj >= ny) continue;
-                f.pc[gi + nx * gj] = s0[b * W + a];
+                bp[pcur ^ 1][gi + nx * gj] = s0[b * W + a];
             }
+            pcur ^= 1;
             block_partials<KS, 2 * KS, NT>(&wred[0][0], partials, G);
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
             reduce_partials<KS, NT>(partials, G, tot);
@@ -445,12 +455,21 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         }
         if (failed) break;
 
+        T *const pcc = bp[pcur];  // the current p'
+        if (npass_p == 0) {       // no p' sweeps: p' = 0 (src/Solver.cu:193)
+            for (int q = tid; q < TX * TY; q += NT) {
+                const int i = x0 + q % TX, j = y0 + q / TX;
+                if (i < nx && j < ny) pcc[i + nx * j] = (T)0;
+            }
+            if (!grid_sync(bar, G, epoch)) break;
+        }
+
         // -------- optional p' mean removal (closed domains, FP64) --------
         if (pa.pin) {
             double m[1] = {0.0};
             for (int q = tid; q < TX * TY; q += NT) {
                 const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i < nx && j < ny) m[0] += (double)f.pc[i + nx * j];
+                if (i < nx && j < ny) m[0] += (double)pcc[i + nx * j];
             }
             write_partials<1, NT>(m, partials, G);
             if (!grid_sync(bar, G, epoch)) break;
@@ -458,7 +477,7 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
             const double mean = tot[0] / (double)N;
             for (int q = tid; q < TX * TY; q += NT) {
                 const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i < nx && j < ny) f.pc[i + nx * j] = (T)((double)f.pc[i + nx * j] - mean);
+                if (i < nx && j < ny) pcc[i + nx * j] = (T)((double)pcc[i + nx * j] - mean);
             }
             if (!grid_sync(bar, G, epoch)) break;
         }
@@ -472,11 +491,11 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 const int c = i + nx * j;
                 const int fu = i + (nx + 1) * j;
                 // loads first
-                const T pc = f.pc[c], aC = f.ac[c];
-                const T pcW = i > 0 ? f.pc[c - 1] : (T)0, pcE = i < nx - 1 ? f.pc[c + 1] : (T)0;
-                const T pcS = j > 0 ? f.pc[c - nx] : (T)0, pcN = j < ny - 1 ? f.pc[c + nx] : (T)0;
+                const T pc = pcc[c], aC = f.ac[c];
+                const T pcW = i > 0 ? pcc[c - 1] : (T)0, pcE = i < nx - 1 ? pcc[c + 1] : (T)0;
+                const T pcS = j > 0 ? pcc[c - nx] : (T)0, pcN = j < ny - 1 ? pcc[c + nx] : (T)0;
                 const T acW = i > 0 ? f.ac[c - 1] : (T)1, acS = j > 0 ? f.ac[c - nx] : (T)1;
-                const T p0 = f.p[c], u0 = f.u[c], v0 = f.v[c];
+                const T p0 = f.p[c], u0 = fc.u[c], v0 = fc.v[c];
                 const T uf0 = i > 0 ? f.uf[fu] : (T)0, vf0 = j > 0 ? f.vf[c] : (T)0;
                 const T dp = g.relax[EQ_P] * pc;
                 const T L_ = i > 0 ? pcW : (g.closed[WEST] ? pc : (T)0);
@@ -489,6 +508,7 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 f.p[c] = p0 + dp;
                 f.u[c] = un;
                 f.v[c] = vn;
+                if (pcc != f.pc) f.pc[c] = pc;  // keep the p' field current for readers
                 s[0] += (double)dp * (double)dp;
                 s[1] += (double)du * (double)du;
                 s[2] += (double)dv * (double)dv;

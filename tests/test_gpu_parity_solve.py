@@ -126,3 +126,23 @@ def test_device_matches_reference_build(gpu_ok, name, closed):
     if closed:
         p, pr = p - p.mean(), pr - pr.mean()
     assert rel_l2(p, pr) < 1e-5, rel_l2(p, pr)
+
+
+@pytest.mark.parametrize("sweeps_per_pass", [5, 4, 3])
+def test_fused_graph_path_with_more_tiles_than_resident_ctas(gpu_ok, sweeps_per_pass):
+    """A 1024 x 512 channel has far more 32 x 16 tiles than CTAs resident at
+    once, so it runs the graph of fused passes, whose later tiles start after
+    earlier ones have finished.  Each pass stages halos from one buffer and
+    writes to the other, so the result equals global red-black sweeps exactly;
+    4 sweeps per pass gives an odd number of momentum passes (the final copy)
+    and 3 an odd number of p' passes."""
+    from helpers import assert_bitwise
+
+    cfg = ifc.channel2d(1024, 512, sweeps_per_pass=sweeps_per_pass)
+    s = ifc.Solver(cfg)
+    s.iterate(2)
+    oc = to_oracle_cfg(cfg)
+    o = O.Oracle(oc, "f")
+    o.solve(2)
+    for k in ("u", "v", "p", "uf", "vf"):
+        assert_bitwise(s.get(k), o.field(k), k)
