@@ -560,12 +560,22 @@ def run_batch(args):
     cases = ifc.batch_cases(args.cases, seed=0)
     mine = ifc.shard_cases([c["nx"] * c["ny"] for c in cases], rank, world) if world > 1 else list(range(len(cases)))
     sub = [cases[i] for i in mine]
-    # warm-up on a few small cases
-    ifc.batch_solve([ifc.cavity2d(32)] * 4, want_fields=False)
+    # warm-up: one case of every size class, which also runs the autotuner
+    # (it times each variant once per class and process); its time is reported
+    t0 = time.perf_counter()
+    ifc.batch_solve([ifc.cavity2d(32), ifc.cavity2d(128), ifc.cavity2d(256)], want_fields=False)
+    tune_s = time.perf_counter() - t0
     clocks = ClockSampler(local)
     clocks.start()
     res, fields, bms = ifc.batch_solve(sub)
     clk = clocks.stop()
+    case_its = sum(r["outer_iterations"] for r in res)
+    updates = sum(r["outer_iterations"] * c["nx"] * c["ny"] * (c["nIter_u"] + c["nIter_v"] + c["nIter_p"])
+                  for r, c in zip(res, sub))
+    variants = {}
+    for r, c in zip(res, sub):
+        key = f"{r['tile_x']}x{r['tile_y']}/ks{r['sweeps_per_pass']}" if r["tile_x"] else "rows/ks1"
+        variants[key] = variants.get(key, 0) + 1
     plain_ms, worst, nconv_b, nconv_p = 0.0, 0.0, 0, 0
     for k, c in enumerate(sub):
         s = ifc.Solver(c)
@@ -588,6 +598,10 @@ def run_batch(args):
         "plain_loop": {"solves_per_s": len(sub) / (plain_ms * 1e-3), "device_ms": plain_ms,
                        "note": "sum of per-case ifc_solve device times, handle creation excluded"},
         "speedup_vs_plain": plain_ms / bms,
+        "case_outer_iterations": case_its,
+        "cell_updates_per_s": updates / (bms * 1e-3),
+        "variants_used": variants,
+        "autotune_and_warmup_seconds": tune_s,
         "converged": {"batch": nconv_b, "plain": nconv_p, "of": len(sub)},
         "max_rel_l2_batch_vs_plain_uv": worst,
         "clocks": clk,

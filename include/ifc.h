@@ -163,14 +163,21 @@ typedef struct ifc_batch_result {
     int converged;
     int sweeps[4];                    /* u v w p' sweeps of the last outer iteration */
     double rel_p, rel_u, rel_v, rel_uf, rel_vf, norm_mass;
+    int tile_x, tile_y;               /* tile shape the case ran with (0 0: whole-row sweeps) */
+    int sweeps_per_pass;              /* sweeps between the inner early-exit checks */
 } ifc_batch_result;
 
 /* Solves n independent 2D cases (each a full ifc_config: its own grid, fluid,
  * boundary conditions and iteration counts; all 2D, Gauss-Seidel, one
- * precision) to convergence or num_outer_iter, in one persistent kernel of
+ * precision) to convergence or num_outer_iter, in persistent kernels of
  * thread-block clusters that take cases from a device queue, relaunched by a
  * CUDA graph until every case has finished.  Each case runs the same SIMPLE
- * iteration as ifc_solve with the per-field convergence rule.  results: n
+ * iteration as ifc_solve.  A case's size class (up to 64^2, 160^2, larger
+ * cells) selects how its sweeps run: whole-row sweeps, or temporally blocked
+ * passes of a tile shape and sweeps per pass; the first batch of a process
+ * that meets a class times every variant on copies of the class's median case
+ * and keeps the fastest for the rest of the process (IFC_BATCH_VARIANT=<k> in
+ * the environment forces variant k).  results: n
  * entries.  fields_out (optional): n host pointers, each receiving u, v, p of
  * its case (3*nx*ny values of the case's precision), or NULL entries.
  * device_ms (optional): device time of the whole batch.  Device memory is

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cooperative_groups.h>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -456,6 +457,84 @@ __global__ void __cluster_dims__(kCL, 1, 1) __launch_bounds__(kBNT, 4)
     }
 }
 
+#include "ifc_batch_tb.cuh"
+
+// ---- variants and the autotuner ---------------------------------------------
+// Variant 0 sweeps whole rows with one cluster barrier per half sweep
+// (k_batch2d); the others are temporally blocked (k_batch_tb) with the tile
+// shape and sweeps per pass of the table.  A case's size class selects its
+// variant: the autotuner times every variant on copies of the class's median
+// case (a fixed number of outer iterations) the first time a class is met in a
+// process, and keeps the fastest.  IFC_BATCH_VARIANT=<k> forces variant k.
+struct BVariant {
+    int tx, ty, ks, nt;
+};
+constexpr int kNumVariants = 3;
+constexpr BVariant kVariants[kNumVariants] = {{0, 0, 1, kBNT}, {32, 8, 3, 256}, {32, 16, 5, 512}};
+constexpr int kNumClasses = 3;
+
+static int size_class(int nx, int ny)
+{
+    const long long cells = (long long)nx * ny;
+    return cells <= 64 * 64 ? 0 : (cells <= 160 * 160 ? 1 : 2);
+}
+
+template <typename T>
+static const void *variant_kernel(int v)
+{
+    switch (v) {
+    case 1: return (const void *)k_batch_tb<T, 32, 8, 3, 256>;
+    case 2: return (const void *)k_batch_tb<T, 32, 16, 5, 512>;
+    default: return (const void *)k_batch2d<T>;
+    }
+}
+
+template <typename T>
+static size_t variant_smem(int v)
+{
+    const BVariant &b = kVariants[v];
+    if (b.tx == 0) return 0;
+    const int W = b.tx + 4 * b.ks, HH = b.ty + 4 * b.ks;
+    return (size_t)3 * W * HH * sizeof(T);
+}
+
+template <typename T>
+static cudaError_t variant_clusters(int v, int *nclusters)
+{
+    const void *kern = variant_kernel<T>(v);
+    const size_t smem = variant_smem<T>(v);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(kCL);
+    lc.blockDim = dim3(kVariants[v].nt);
+    lc.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kCL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(nclusters, kern, &lc);
+}
+
+template <typename T>
+static void launch_variant(int v, int nclusters, cudaStream_t st, const BCase<T> *dc, BState *ds, BPools<T> pool,
+                           TBPools<T> tp, int n, BQueue *dq, int chunk, cudaGraphConditionalHandle cond)
+{
+    const size_t smem = variant_smem<T>(v);
+    switch (v) {
+    case 1:
+        k_batch_tb<T, 32, 8, 3, 256><<<nclusters * kCL, 256, smem, st>>>(dc, ds, pool, tp, n, dq, chunk, cond, 1);
+        break;
+    case 2:
+        k_batch_tb<T, 32, 16, 5, 512><<<nclusters * kCL, 512, smem, st>>>(dc, ds, pool, tp, n, dq, chunk, cond, 1);
+        break;
+    default: k_batch2d<T><<<nclusters * kCL, kBNT, 0, st>>>(dc, ds, pool, n, dq, chunk, cond, 1); break;
+    }
+}
+
 #define BCK(call)                                                                  \
     do {                                                                           \
         if ((call) != cudaSuccess) {                                               \
@@ -465,11 +544,78 @@ __global__ void __cluster_dims__(kCL, 1, 1) __launch_bounds__(kBNT, 4)
     } while (0)
 
 template <typename T>
-int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *const *fields_out, double *ms_out)
+static int batch_run(const ifc_config *cfgs, int n, int force_variant, ifc_batch_result *res, void *const *fields_out,
+                     double *ms_out);
+
+// Variant chosen for each size class and precision in this process.
+static std::mutex g_tune_mu;
+static int g_tuned[2][kNumClasses] = {{-1, -1, -1}, {-1, -1, -1}};
+
+template <typename T>
+static int autotune(int cls, const ifc_config &rep)
+{
+    // Probe: copies of the class's median case, 20 outer iterations each (no
+    // early stop), enough copies to fill the GPU with any variant.
+    constexpr int kCopies = 96;
+    std::vector<ifc_config> probe(kCopies, rep);
+    for (ifc_config &c : probe) {
+        c.tol_u = c.tol_v = c.tol_w = c.tol_p = 0.0;
+        c.tol_mass = 0.0;
+        c.num_outer_iter = 20;
+    }
+    std::vector<ifc_batch_result> r(kCopies);
+    int best = 0;
+    double best_ms = 0.0;
+    for (int v = 0; v < kNumVariants; ++v) {
+        double ms = 0.0;
+        if (batch_run<T>(probe.data(), kCopies, v, r.data(), nullptr, &ms) != IFC_OK) continue;
+        if (getenv("IFC_VERBOSE"))
+            fprintf(stderr, "ifc_batch autotune: class %d (%dx%d) variant %d: %.3f ms\n", cls, rep.nx, rep.ny, v, ms);
+        if (best_ms == 0.0 || ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    return best;
+}
+
+template <typename T>
+static int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *const *fields_out, double *ms_out)
+{
+    const char *env = getenv("IFC_BATCH_VARIANT");
+    if (env && env[0] >= '0' && env[0] < '0' + kNumVariants)
+        return batch_run<T>(cfgs, n, env[0] - '0', res, fields_out, ms_out);
+    const int prec = sizeof(T) == 8 ? 1 : 0;
+    for (int cls = 0; cls < kNumClasses; ++cls) {
+        std::vector<int> members;
+        for (int c = 0; c < n; ++c)
+            if (size_class(cfgs[c].nx, cfgs[c].ny) == cls) members.push_back(c);
+        if (members.empty()) continue;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            if (g_tuned[prec][cls] >= 0) continue;
+        }
+        std::sort(members.begin(), members.end(), [&](int x, int y) {
+            return (long long)cfgs[x].nx * cfgs[x].ny < (long long)cfgs[y].nx * cfgs[y].ny;
+        });
+        const int v = autotune<T>(cls, cfgs[members[members.size() / 2]]);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[prec][cls] = v;
+    }
+    return batch_run<T>(cfgs, n, -1, res, fields_out, ms_out);
+}
+
+// Solves the cases; force_variant >= 0 runs every case with that variant,
+// otherwise each size class runs its tuned variant, largest class first, each
+// class as one persistent launch relaunched by a CUDA graph WHILE node.
+template <typename T>
+static int batch_run(const ifc_config *cfgs, int n, int force_variant, ifc_batch_result *res, void *const *fields_out,
+                     double *ms_out)
 {
     int rc = IFC_OK;
+    const int prec = sizeof(T) == 8 ? 1 : 0;
     std::vector<BCase<T>> hc(n);
-    std::vector<int> order(n);
+    std::vector<int> variant(n);
     long long nc = 0, nuf = 0, nvf = 0;
     for (int c = 0; c < n; ++c) {
         BCase<T> &b = hc[c];
@@ -489,28 +635,54 @@ int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *cons
         for (int f = 0; f < 4; ++f) closed = closed && cfgs[c].vel_bc_type[f] != IFC_OUTLET;
         b.pin = cfgs[c].pin_pressure == 1 || (cfgs[c].pin_pressure < 0 && closed);
         b.max_outer = cfgs[c].num_outer_iter;
+        if (force_variant >= 0) {
+            variant[c] = force_variant;
+        } else {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            const int v = g_tuned[prec][size_class(cfgs[c].nx, cfgs[c].ny)];
+            variant[c] = v < 0 ? 0 : v;
+        }
     }
-    // Queue order: largest grids first (longest-processing-time heuristic).
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        return (long long)cfgs[a].nx * cfgs[a].ny > (long long)cfgs[b].nx * cfgs[b].ny;
-    });
+    // One queue per variant, largest grids first (longest-processing-time
+    // heuristic); the queue with the most work runs first.
+    std::vector<std::vector<int>> groups(kNumVariants);
+    std::vector<long long> work(kNumVariants, 0);
+    for (int c = 0; c < n; ++c) {
+        groups[variant[c]].push_back(c);
+        work[variant[c]] += (long long)cfgs[c].nx * cfgs[c].ny;
+    }
+    std::vector<int> vorder;
+    for (int v = 0; v < kNumVariants; ++v)
+        if (!groups[v].empty()) vorder.push_back(v);
+    std::sort(vorder.begin(), vorder.end(), [&](int x, int y) { return work[x] > work[y]; });
+    std::vector<int> order;  // queue position -> case
+    std::vector<int> qbegin, qsize;
+    for (int v : vorder) {
+        std::vector<int> &g = groups[v];
+        std::stable_sort(g.begin(), g.end(), [&](int x, int y) {
+            return (long long)cfgs[x].nx * cfgs[x].ny > (long long)cfgs[y].nx * cfgs[y].ny;
+        });
+        qbegin.push_back((int)order.size());
+        qsize.push_back((int)g.size());
+        order.insert(order.end(), g.begin(), g.end());
+    }
     std::vector<BCase<T>> queued(n);
     for (int k = 0; k < n; ++k) queued[k] = hc[order[k]];
 
     BPools<T> pool;
     std::memset(&pool, 0, sizeof(pool));
+    TBPools<T> tp = {nullptr, nullptr, nullptr};
     BCase<T> *dcases = nullptr;
     BState *dstates = nullptr;
     BQueue *dq = nullptr;
     cudaStream_t st = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaGraph_t> graphs;
+    std::vector<cudaGraphExec_t> execs;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::vector<BState> hs(n);
     {
         T **cell_arrays[] = {&pool.u, &pool.v, &pool.p, &pool.pc, &pool.ac, &pool.rac, &pool.sp,
-                             &pool.le, &pool.ln, &pool.lc};
+                             &pool.le, &pool.ln, &pool.lc, &tp.tu, &tp.tv, &tp.tpc};
         for (T **a : cell_arrays) {
             BCK(cudaMalloc(a, nc * sizeof(T)));
             BCK(cudaMemset(*a, 0, nc * sizeof(T)));
@@ -528,32 +700,24 @@ int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *cons
         BCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         BCK(cudaEventCreate(&e0));
         BCK(cudaEventCreate(&e1));
-
-        // Persistent grid: as many 8-CTA clusters as fit at once.
-        int nclusters = 0;
-        {
-            cudaLaunchConfig_t lc = {};
-            lc.gridDim = dim3(kCL);
-            lc.blockDim = dim3(kBNT);
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = kCL;
-            at[0].val.clusterDim.y = 1;
-            at[0].val.clusterDim.z = 1;
-            lc.attrs = at;
-            lc.numAttrs = 1;
-            BCK(cudaOccupancyMaxActiveClusters(&nclusters, (void *)k_batch2d<T>, &lc));
-        }
-        if (nclusters < 1) nclusters = 1;
-        if (nclusters > n) nclusters = n;
-        if (getenv("IFC_VERBOSE")) fprintf(stderr, "ifc_batch_solve: %d clusters of %d CTAs\n", nclusters, kCL);
         const int chunk = 250;
 
-        // CUDA graph: WHILE (any case unfinished) { k_batch2d }
-        cudaGraphConditionalHandle cond;
-        BCK(cudaGraphCreate(&graph, 0));
-        BCK(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
-        {
+        // One graph per queue: WHILE (a case of the queue is unfinished) { kernel }
+        for (size_t gq = 0; gq < vorder.size(); ++gq) {
+            const int v = vorder[gq];
+            int nclusters = 0;
+            BCK(variant_clusters<T>(v, &nclusters));
+            if (nclusters < 1) nclusters = 1;
+            if (nclusters > qsize[gq]) nclusters = qsize[gq];
+            if (getenv("IFC_VERBOSE"))
+                fprintf(stderr, "ifc_batch_solve: queue of %d cases, variant %d, %d clusters of %d CTAs\n", qsize[gq],
+                        v, nclusters, kCL);
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            cudaGraphConditionalHandle cond;
+            BCK(cudaGraphCreate(&graph, 0));
+            graphs.push_back(graph);
+            BCK(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
             cudaGraphNodeParams cp = {};
             cp.type = cudaGraphNodeTypeConditional;
             cp.conditional.handle = cond;
@@ -563,12 +727,14 @@ int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *cons
             BCK(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
             cudaGraph_t body = cp.conditional.phGraph_out[0];
             BCK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-            k_batch2d<T><<<nclusters * kCL, kBNT, 0, st>>>(dcases, dstates, pool, n, dq, chunk, cond, 1);
+            launch_variant<T>(v, nclusters, st, dcases + qbegin[gq], dstates + qbegin[gq], pool, tp, qsize[gq], dq,
+                              chunk, cond);
             BCK(cudaStreamEndCapture(st, &body));
+            BCK(cudaGraphInstantiate(&exec, graph, 0));
+            execs.push_back(exec);
         }
-        BCK(cudaGraphInstantiate(&exec, graph, 0));
         BCK(cudaEventRecord(e0, st));
-        BCK(cudaGraphLaunch(exec, st));
+        for (cudaGraphExec_t x : execs) BCK(cudaGraphLaunch(x, st));
         BCK(cudaEventRecord(e1, st));
         BCK(cudaStreamSynchronize(st));
         BCK(cudaGetLastError());
@@ -591,6 +757,10 @@ int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *cons
             r.rel_uf = s.rel[4];
             r.rel_vf = s.rel[5];
             r.norm_mass = s.norm[7];
+            const BVariant &bv = kVariants[variant[c]];
+            r.tile_x = bv.tx;
+            r.tile_y = bv.ty;
+            r.sweeps_per_pass = bv.ks;
             if (fields_out && fields_out[c]) {
                 const size_t cells = (size_t)cfgs[c].nx * cfgs[c].ny;
                 T *out = (T *)fields_out[c];
@@ -601,13 +771,15 @@ int batch_solve(const ifc_config *cfgs, int n, ifc_batch_result *res, void *cons
         }
     }
 done:
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    for (cudaGraphExec_t x : execs)
+        if (x) cudaGraphExecDestroy(x);
+    for (cudaGraph_t gph : graphs)
+        if (gph) cudaGraphDestroy(gph);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st) cudaStreamDestroy(st);
     T *all[] = {pool.u, pool.v, pool.p, pool.pc, pool.ac, pool.rac, pool.sp, pool.uf, pool.vf,
-                pool.le, pool.ln, pool.lc};
+                pool.le, pool.ln, pool.lc, tp.tu, tp.tv, tp.tpc};
     for (T *a : all)
         if (a) cudaFree(a);
     if (dcases) cudaFree(dcases);

@@ -69,7 +69,8 @@ class IfcStats(C.Structure):
 class IfcBatchResult(C.Structure):
     _fields_ = [("status", C.c_int), ("outer_iterations", C.c_int), ("converged", C.c_int),
                 ("sweeps", C.c_int * 4)] + [(n, C.c_double) for n in (
-                    "rel_p", "rel_u", "rel_v", "rel_uf", "rel_vf", "norm_mass")]
+                    "rel_p", "rel_u", "rel_v", "rel_uf", "rel_vf", "norm_mass")] + [
+                ("tile_x", C.c_int), ("tile_y", C.c_int), ("sweeps_per_pass", C.c_int)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_ if n != "sweeps"}

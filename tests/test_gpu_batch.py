@@ -1,10 +1,13 @@
 """The batched form (ifc_batch_solve): many independent 2D cases of uneven
 size, Reynolds number and boundary type in one persistent launch, each checked
 against the CPU oracle run on its own (same red-black ordering, inner
-early-exit rule after every sweep).  Tolerance: relative L2 1e-6 against the
-oracle with the same ordering (FP64 norms summed in a different order can move
-a convergence decision by one iteration), and the north star's 1e-4 against
-the FP64 lexicographic oracle."""
+early-exit rule at the granularity the case ran with: after every sweep for
+whole-row sweeps, after every pass of sweeps_per_pass sweeps for the
+temporally blocked variants).  Every variant is run forced
+(IFC_BATCH_VARIANT) and as chosen by the autotuner.  Tolerance: relative L2
+1e-6 against the oracle with the same ordering (FP64 norms summed in a
+different order can move a convergence decision by one iteration), and the
+north star's 1e-4 against the FP64 lexicographic oracle."""
 import numpy as np
 import pytest
 
@@ -23,19 +26,30 @@ def mixed_cases():
     return cases
 
 
-def oracle_fields(cfg, sweep_mode=O.GS_REDBLACK, prec="f"):
-    o = O.Oracle(to_oracle_cfg(dict(cfg, sweep_mode=sweep_mode, check_every=1)), prec)
+def oracle_fields(cfg, sweep_mode=O.GS_REDBLACK, prec="f", check_every=1):
+    o = O.Oracle(to_oracle_cfg(dict(cfg, sweep_mode=sweep_mode, check_every=check_every)), prec)
     n, nm = o.solve()
     p = o.field("p").astype(np.float64)
     return n, nm, {"u": o.field("u").copy(), "v": o.field("v").copy(), "p": p}
 
 
-def test_batch_matches_oracle(gpu_ok):
+@pytest.fixture(params=["0", "1", "2", "tuned"])
+def batch_variant(request, monkeypatch):
+    if request.param == "tuned":
+        monkeypatch.delenv("IFC_BATCH_VARIANT", raising=False)
+    else:
+        monkeypatch.setenv("IFC_BATCH_VARIANT", request.param)
+    return request.param
+
+
+def test_batch_matches_oracle(gpu_ok, batch_variant):
     cases = mixed_cases()
     res, fields, ms = ifc.batch_solve(cases)
     assert ms > 0
     for c, r, f in zip(cases, res, fields):
-        n, nm, ref = oracle_fields(c)
+        if batch_variant != "tuned":
+            assert r["sweeps_per_pass"] == {"0": 1, "1": 3, "2": 5}[batch_variant]
+        n, nm, ref = oracle_fields(c, check_every=r["sweeps_per_pass"])
         assert r["converged"] == nm["converged"] == 1, (r, nm)
         assert abs(r["outer_iterations"] - n) <= 1, (r["outer_iterations"], n)
         closed = all(t != ifc.OUTLET for t in c["velBC_type"][:4])
@@ -46,7 +60,7 @@ def test_batch_matches_oracle(gpu_ok):
             assert rel_l2(a, b) < 1e-6, (c["nx"], c["ny"], k, rel_l2(a, b))
 
 
-def test_batch_is_deterministic_and_order_independent(gpu_ok):
+def test_batch_is_deterministic_and_order_independent(gpu_ok, batch_variant):
     cases = mixed_cases()
     r1, f1, _ = ifc.batch_solve(cases)
     r2, f2, _ = ifc.batch_solve(list(reversed(cases)))
@@ -59,7 +73,7 @@ def test_batch_is_deterministic_and_order_independent(gpu_ok):
 def test_batch_case_against_fp64_oracle(gpu_ok):
     c = ifc.cavity2d(32, re=100.0)
     res, fields, _ = ifc.batch_solve([c])
-    _, _, ref = oracle_fields(c, O.GS_LEX, "d")
+    _, _, ref = oracle_fields(c, O.GS_LEX, "d", res[0]["sweeps_per_pass"])
     for k in ("u", "v", "p"):
         a, b = fields[0][k].astype(np.float64), ref[k]
         if k == "p":
