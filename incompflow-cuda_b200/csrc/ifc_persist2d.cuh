@@ -54,8 +54,11 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks, 
     if (threadIdx.x == 0) {
         int good = 1;
         const unsigned int target = epoch * nblocks;
-        __threadfence();
-        const unsigned int old = atomicAdd(&b->count, 1u);
+        // The arrival releases this CTA's writes (ordered before it by the
+        // __syncthreads above) and, for the last CTA to arrive, acquires the
+        // others'; the pollers acquire them through ld.acquire.
+        unsigned int old;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(&b->count) : "memory");
         if (old + 1 < target) {
             const unsigned long long t0 = global_ns();
             unsigned int spins = 0;
@@ -69,7 +72,6 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks, 
             }
         }
         if (*(volatile int *)&b->err) good = 0;
-        __threadfence();
         ok = good;
     }
     __syncthreads();
@@ -77,37 +79,20 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks, 
 }
 
 // Sum column r of partials (one value per CTA) for r < NRV in a fixed order;
-// identical in every CTA.  All loads are issued before any reduction so the
-// columns cost one round trip to L2 together.  out: shared, NRV entries.
+// identical in every CTA.  Warp w sums columns w, w + NT/32, ... (each
+// lane-strided, then one shuffle tree), so the columns are reduced in
+// parallel with one round trip to L2.  out: shared, NRV entries.
 template <int NRV, int NT>
 __device__ __forceinline__ void reduce_partials(const double *partials, int G, double *out)
 {
-    __shared__ double red[NT / 32][NRV];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double x[NRV];
-#pragma unroll
-    for (int r = 0; r < NRV; ++r) x[r] = 0.0;
-    for (int b0 = 0; b0 < G; b0 += NT) {
-        const int b = b0 + threadIdx.x;
-        double y[NRV];
-#pragma unroll
-        for (int r = 0; r < NRV; ++r) y[r] = b < G ? __ldcg(&partials[(size_t)r * G + b]) : 0.0;
-#pragma unroll
-        for (int r = 0; r < NRV; ++r) x[r] += y[r];
-    }
-#pragma unroll
-    for (int r = 0; r < NRV; ++r) {
-        const double t = warp_sum(x[r]);
-        if (lane == 0) red[warp][r] = t;
-    }
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int r = 0; r < NRV; ++r) {
-            double t = lane < NT / 32 ? red[lane][r] : 0.0;
-            t = warp_sum(t);
-            if (lane == 0) out[r] = t;
-        }
+    for (int r = warp; r < NRV; r += NT / 32) {
+        const double *col = partials + (size_t)r * G;
+        double x = 0.0;
+#pragma unroll 4
+        for (int b = lane; b < G; b += 32) x += __ldcg(&col[b]);
+        x = warp_sum(x);
+        if (lane == 0) out[r] = x;
     }
     __syncthreads();
 }
@@ -177,6 +162,15 @@ __device__ __forceinline__ void pass_done(LoopState &L, int e, const double *sq,
     L.sweeps[e] += ns;
     L.cell_updates += (long long)ns * N;
     if (stop_now) L.stop[e] = 1;
+}
+
+// Bookkeeping of the last pass of a phase: its sums could only set an
+// early-exit flag for passes that do not follow (the flags are reset with
+// every outer iteration), so they are not reduced.
+__device__ __forceinline__ void pass_count(LoopState &L, int e, int ns, int N)
+{
+    L.sweeps[e] += ns;
+    L.cell_updates += (long long)ns * N;
 }
 
 template <typename T, int TX, int TY, int KS, int NT>
@@ -341,12 +335,19 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 bv[mcur ^ 1][id] = s1[b * W + a];
             }
             mcur ^= 1;
-            block_partials<2 * KS, 2 * KS, NT>(&wred[0][0], partials, G);
+            const bool last = pass >= npass_m - 1;
+            if (!last) block_partials<2 * KS, 2 * KS, NT>(&wred[0][0], partials, G);
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
-            reduce_partials<2 * KS, NT>(partials, G, tot);
+            if (!last) reduce_partials<2 * KS, NT>(partials, G, tot);
             if (tid == 0) {
-                if (au) pass_done(L, EQ_U, tot, ns[0], N, g.tol[EQ_U]);
-                if (av) pass_done(L, EQ_V, tot + KS, ns[1], N, g.tol[EQ_V]);
+                if (au) {
+                    if (last) pass_count(L, EQ_U, ns[0], N);
+                    else pass_done(L, EQ_U, tot, ns[0], N, g.tol[EQ_U]);
+                }
+                if (av) {
+                    if (last) pass_count(L, EQ_V, ns[1], N);
+                    else pass_done(L, EQ_V, tot + KS, ns[1], N, g.tol[EQ_V]);
+                }
             }
             __syncthreads();
         }
@@ -447,10 +448,14 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 bp[pcur ^ 1][gi + nx * gj] = s0[b * W + a];
             }
             pcur ^= 1;
-            block_partials<KS, 2 * KS, NT>(&wred[0][0], partials, G);
+            const bool last = pass == npass_p - 1;
+            if (!last) block_partials<KS, 2 * KS, NT>(&wred[0][0], partials, G);
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
-            reduce_partials<KS, NT>(partials, G, tot);
-            if (tid == 0) pass_done(L, EQ_P, tot, ns, N, g.tol[EQ_P]);
+            if (!last) reduce_partials<KS, NT>(partials, G, tot);
+            if (tid == 0) {
+                if (last) pass_count(L, EQ_P, ns, N);
+                else pass_done(L, EQ_P, tot, ns, N, g.tol[EQ_P]);
+            }
             __syncthreads();
         }
         if (failed) break;
