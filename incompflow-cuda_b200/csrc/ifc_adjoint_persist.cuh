@@ -91,40 +91,22 @@ __device__ __forceinline__ void smm_partials(double s, double m1, double m2, dou
 template <int NT>
 __device__ __forceinline__ void smm_reduce(const double *partials, int G, double *out)
 {
-    __shared__ double red[NT / 32][3];
+    // warp 0: sum of column 0; warps 1, 2: max of columns 1, 2 (lane-strided,
+    // then one shuffle tree: a fixed order, identical in every CTA)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double s = 0.0, m1 = 0.0, m2 = 0.0;
-    for (int b0 = 0; b0 < G; b0 += NT) {
-        const int b = b0 + threadIdx.x;
-        const double y0 = b < G ? __ldcg(&partials[b]) : 0.0;
-        const double y1 = b < G ? __ldcg(&partials[G + b]) : 0.0;
-        const double y2 = b < G ? __ldcg(&partials[2 * G + b]) : 0.0;
-        s += y0;
-        m1 = fmax(m1, y1);
-        m2 = fmax(m2, y2);
-    }
-    s = warp_sum(s);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        m1 = fmax(m1, __shfl_down_sync(0xffffffffu, m1, o));
-        m2 = fmax(m2, __shfl_down_sync(0xffffffffu, m2, o));
-    }
-    if (lane == 0) {
-        red[warp][0] = s;
-        red[warp][1] = m1;
-        red[warp][2] = m2;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int w = 0; w < NT / 32; ++w) {
-            a0 += red[w][0];
-            a1 = fmax(a1, red[w][1]);
-            a2 = fmax(a2, red[w][2]);
+    if (warp < 3) {
+        const double *col = partials + (size_t)warp * G;
+        double x = 0.0;
+        for (int b = lane; b < G; b += 32) {
+            const double y = __ldcg(&col[b]);
+            x = warp == 0 ? x + y : fmax(x, y);
         }
-        out[0] = a0;
-        out[1] = a1;
-        out[2] = a2;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_down_sync(0xffffffffu, x, o);
+            x = warp == 0 ? x + y : fmax(x, y);
+        }
+        if (lane == 0) out[warp] = x;
     }
     __syncthreads();
 }

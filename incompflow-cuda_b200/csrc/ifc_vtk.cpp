@@ -3,9 +3,11 @@
 //
 // The reference streams every value through std::ostream with the default
 // format (6 significant digits, %g style) followed by a space.  This writer
-// formats with snprintf("%g") into per-thread buffers and writes them in
-// order, so the bytes are the same and large grids are formatted in parallel.
+// produces the same bytes with its own formatter (fmt_g6, below; snprintf for
+// the cases it cannot decide) into per-thread buffers written in order, so
+// large grids are formatted in parallel.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -16,20 +18,96 @@
 
 namespace {
 
+// Exact powers of ten representable in double.
+const double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                           1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+// snprintf("%g", x) (precision 6, no flags) for finite x, in the C locale:
+// 6 significant digits rounded to nearest, %e style when the decimal exponent
+// X is < -4 or >= 6, else %f style, trailing zeros and a bare decimal point
+// removed.  The 6 digits are x * 10^(5-X) rounded, computed with one double
+// multiplication by an exact power of ten; when the product lies within 1e-7
+// of a rounding tie (or the exponent needs an inexact power) the exact
+// decimal value decides, so this defers to snprintf.  Returns the length.
+int fmt_g6(double x, char *out)
+{
+    if (!std::isfinite(x)) return std::snprintf(out, 32, "%g", x);
+    char *o = out;
+    if (std::signbit(x)) {
+        *o++ = '-';
+        x = -x;
+    }
+    if (x == 0.0) {
+        *o++ = '0';
+        return (int)(o - out);
+    }
+    int e2;
+    std::frexp(x, &e2);
+    int X = (int)std::floor((e2 - 1) * 0.30102999566398120);  // floor(log10(x)), or one below
+    if (X + 1 <= 308 && x >= (X + 1 >= 0 && X + 1 <= 22 ? kPow10[X + 1] : std::pow(10.0, X + 1))) ++X;
+    const int k = 5 - X;
+    if (k < -22 || k > 22) return (int)(o - out) + std::snprintf(o, 32, "%g", x);
+    const double m = k >= 0 ? x * kPow10[k] : x / kPow10[-k];
+    double fl = std::floor(m);
+    const double fr = m - fl;
+    if (std::fabs(fr - 0.5) < 1e-7) return (int)(o - out) + std::snprintf(o, 32, "%g", x);
+    long long n = (long long)fl + (fr > 0.5 ? 1 : 0);
+    if (n < 100000) {  // X was one too high (cannot happen after the check above; be safe)
+        return (int)(o - out) + std::snprintf(o, 32, "%g", x);
+    }
+    if (n >= 1000000) {  // rounded up to the next power of ten
+        n /= 10;
+        ++X;
+    }
+    char d[6];
+    for (int q = 5; q >= 0; --q) {
+        d[q] = (char)('0' + n % 10);
+        n /= 10;
+    }
+    int last = 5;  // last significant digit after removing trailing zeros
+    while (last > 0 && d[last] == '0') --last;
+    if (X < -4 || X >= 6) {
+        *o++ = d[0];
+        if (last > 0) {
+            *o++ = '.';
+            for (int q = 1; q <= last; ++q) *o++ = d[q];
+        }
+        *o++ = 'e';
+        *o++ = X < 0 ? '-' : '+';
+        const int ax = X < 0 ? -X : X;
+        if (ax >= 100) *o++ = (char)('0' + ax / 100);
+        *o++ = (char)('0' + (ax / 10) % 10);
+        *o++ = (char)('0' + ax % 10);
+    } else if (X >= 0) {
+        for (int q = 0; q <= X; ++q) *o++ = d[q];
+        if (last > X) {
+            *o++ = '.';
+            for (int q = X + 1; q <= last; ++q) *o++ = d[q];
+        }
+    } else {
+        *o++ = '0';
+        *o++ = '.';
+        for (int q = 0; q < -X - 1; ++q) *o++ = '0';
+        for (int q = 0; q <= last; ++q) *o++ = d[q];
+    }
+    return (int)(o - out);
+}
+
 template <typename T>
 void append_values(std::string &out, const T *a, const T *b, const T *c, size_t lo, size_t hi)
 {
     char buf[64];
     out.reserve(out.size() + (hi - lo) * (c ? 36 : 12));
     for (size_t q = lo; q < hi; ++q) {
-        int n = std::snprintf(buf, sizeof(buf), "%g ", (double)a[q]);
-        out.append(buf, (size_t)n);
+        int n = fmt_g6((double)a[q], buf);
+        buf[n++] = ' ';
         if (b) {
-            n = std::snprintf(buf, sizeof(buf), "%g ", (double)b[q]);
-            out.append(buf, (size_t)n);
-            n = std::snprintf(buf, sizeof(buf), "%g ", (double)c[q]);
-            out.append(buf, (size_t)n);
+            n += fmt_g6((double)b[q], buf + n);
+            buf[n++] = ' ';
+            n += fmt_g6((double)c[q], buf + n);
+            buf[n++] = ' ';
         }
+        out.append(buf, (size_t)n);
     }
 }
 
@@ -79,7 +157,10 @@ int write_vtk(const ifc_config *cfg, const T *u, const T *v, const T *w, const T
         ok = ok && std::fprintf(fp, "%s %d float\n", A.name, A.n + 1) > 0;
         for (int i = 0; i <= A.n && ok; ++i) {
             const T x = A.lo + (T)i * A.d;
-            ok = std::fprintf(fp, "%g ", (double)x) > 0;
+            char buf[40];
+            const int n = fmt_g6((double)x, buf);
+            buf[n] = ' ';
+            ok = std::fwrite(buf, 1, (size_t)n + 1, fp) == (size_t)n + 1;
         }
         ok = ok && std::fputc('\n', fp) != EOF;
     }

@@ -51,3 +51,38 @@ def test_vtk_bad_path():
     z = np.zeros(16, np.float32)
     with pytest.raises(ifc.IfcError):
         ifc.write_vtk_host(cfg, z, z, z, z, z, "/nonexistent-dir/x.vtk")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_value_formatting_matches_printf_g(prec, tmp_path):
+    """The writer's own %g formatter against Python's correctly rounded '%g'
+    on random bit patterns over the whole exponent range, powers of ten and
+    their neighbours, and values at or near rounding ties."""
+    rng = np.random.default_rng(3)
+    dt = np.float32 if prec == "f" else np.float64
+    ut = np.uint32 if prec == "f" else np.uint64
+    bits = rng.integers(0, np.iinfo(ut).max, 150_000, dtype=np.uint64).astype(ut)
+    vals = [bits.view(dt)]
+    special = []
+    for k in range(-40, 39):
+        for base in (1.0, 9.999995, 9.9999949, 9.9999951, 5.0, 1.000005, 1.234565):
+            v = dt(base * 10.0 ** k)
+            special += [v, np.nextafter(v, dt(np.inf)), np.nextafter(v, dt(-np.inf))]
+    special += [dt(x) for x in (0.0, -0.0, 1234565.0, 999999.5, 99999.95, 1e-4, 1e-5, 9.5e-5, 123456.5, 2.5, 1e6)]
+    vals.append(np.array(special, dt))
+    vals.append((rng.standard_normal(50_000) * 10.0 ** rng.integers(-8, 9, 50_000)).astype(dt))
+    v = np.concatenate(vals)
+    v = v[np.isfinite(v)]
+    nx = 1000
+    ny = -(-v.size // nx)
+    u = np.zeros(nx * ny, dt)
+    u[: v.size] = v
+    z = np.zeros_like(u)
+    cfg = ifc.cavity2d(3, nx=nx, ny=ny, precision=prec)
+    path = str(tmp_path / "fmt.vtk")
+    ifc.write_vtk_host(cfg, u, z, z, z, z, path)
+    txt = open(path).read()
+    got = txt.split("velocity 3")[1].split("\n", 1)[1].split("\npressure")[0].split(" ")[:-1][0::3]
+    ref = ["%g" % float(x) for x in u]
+    bad = [i for i in range(u.size) if got[i] != ref[i]]
+    assert not bad, [(float(u[i]), got[i], ref[i]) for i in bad[:5]]
