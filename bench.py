@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--form", default="plain", choices=["plain", "adjoint", "precision", "batch"],
+    ap.add_argument("--form", default="plain", choices=["plain", "adjoint", "precision", "batch", "convergence"],
                     help="plain: the headline throughput line; adjoint: the differentiation form")
     ap.add_argument("--profiles", type=int, default=32, help="adjoint form: seeded inlet profiles")
     ap.add_argument("--fd-profiles", type=int, default=1,
@@ -610,6 +610,77 @@ def run_batch(args):
         print(json.dumps(line), flush=True)
 
 
+def run_convergence(args):
+    """Time to convergence on the 64^2 lid-driven cavity (Re 100, alpha
+    0.7/0.3, GS 5/5/50, tolerance 1e-5, from rest): this library under the
+    reference's own stopping rule and under the per-field rule, the
+    reference's CUDA build under its own rule (oracle/_ref, one
+    Solver::solve() call from a new Solver, wall clock), and the serial
+    oracle under the per-field rule.  Red-black and the reference's chaotic
+    Gauss-Seidel take different iteration counts, so times are compared at
+    convergence, each by its own count."""
+    import re
+    import numpy as np
+    import torch
+
+    import ifc
+
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    cfg = ifc.cavity2d(64)
+    ours = {}
+    for name, crit in (("reference_rule", ifc.CRIT_REFERENCE), ("per_field_rule", ifc.CRIT_PER_FIELD)):
+        ifc.Solver(dict(cfg, criterion=crit)).solve()  # warm-up (graph build, first launch)
+        runs = []
+        for _ in range(3):
+            s = ifc.Solver(dict(cfg, criterion=crit))
+            st = s.solve()
+            runs.append((st["device_ms"], st["outer_iterations"], st["converged"]))
+            s.close()
+        ms = sorted(r[0] for r in runs)[1]
+        ours[name] = {"ms": ms, "outer_iterations": runs[0][1], "converged": bool(runs[0][2]),
+                      "ms_per_iteration": ms / max(runs[0][1], 1)}
+    ref = {"unavailable": "reference build not present (oracle/_ref)"}
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench_cavity64_converge")
+    if os.path.exists(exe):
+        times, its = [], None
+        for _ in range(3):
+            out = subprocess.run([exe, "0", "1"], capture_output=True, text=True, timeout=600)
+            if out.returncode != 0:
+                break
+            rec = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+            iters = [int(m) for m in re.findall(r"^iter: (\d+)", out.stdout, re.M)]
+            its = iters[-1] if iters else None
+            times.append(rec["step_ms"][0])
+        if times:
+            t = sorted(times)[len(times) // 2]
+            ref = {"ms": t, "outer_iterations": its, "ms_per_iteration": t / its if its else None,
+                   "timing": "wall clock around one Solver::solve() from rest (its own stopping rule)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    from helpers import to_oracle_cfg
+
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    t0 = time.perf_counter()
+    n, nm = o.solve()
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    line = {
+        "metric": "time to convergence", "value": ours["reference_rule"]["ms"] / 1e3, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "steps": 3, "warmup": 1,
+        "ms_per_step": ours["reference_rule"]["ms"], "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: flow from rest",
+        "config": {"workload": "cavity2d_64_re100", "tolerance": 1e-5, "sweeps_u_v_p": [5, 5, 50]},
+        "ours": ours, "reference_cuda_build": ref,
+        "speedup_vs_reference_build": (ref["ms"] / ours["reference_rule"]["ms"]) if "ms" in ref else None,
+        "cpu_baseline": {"value": cpu_ms / 1e3, "unit": "s", "cores": 1, "kind": "port",
+                         "sample": f"serial C oracle, FP32 red-black, per-field rule: {n} outer iterations"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -657,6 +728,8 @@ def main():
         run_precision(args)
     elif args.form == "batch":
         run_batch(args)
+    elif args.form == "convergence":
+        run_convergence(args)
     else:
         run_ours(args)
 
