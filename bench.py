@@ -147,6 +147,19 @@ def profiled_traffic(kernel: str):
     return None
 
 
+def host_cpu() -> str:
+    """CPU model and logical core count of this host (for the baseline label)."""
+    model = "unknown CPU"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{model} ({os.cpu_count()} logical cores)"
+
+
 def cpu_baseline(seconds: float):
     """The serial CPU restatement of the reference's kernels (oracle, FP32,
     1 core) on a bounded sample of the same workload: outer iterations from
@@ -166,8 +179,8 @@ def cpu_baseline(seconds: float):
         updates += o.N * (nm["sweeps"][0] + nm["sweeps"][1] + nm["sweeps"][3])
     dt = time.perf_counter() - t0
     return {"value": updates / dt, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": f"{its} outer iterations of {WORKLOAD} from rest, serial C oracle (FP32, red-black GS), "
-                      f"{dt:.1f} s"}
+            "sample": f"{its} outer iterations of {WORKLOAD} from rest, serial C oracle (FP32, red-black GS, "
+                      f"gcc -O2), {dt:.1f} s on one core of {host_cpu()}"}
 
 
 def dist_env():

@@ -21,6 +21,8 @@
 #include <numeric>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "ifc.h"
 #include "ifc_engine.cuh"
 
@@ -794,6 +796,10 @@ done:
 extern "C" int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result *results, void *const *fields_out,
                                double *device_ms)
 {
+    nvtxRangePushA("ifc_batch_solve");
+    struct Pop {
+        ~Pop() { nvtxRangePop(); }
+    } pop;
     if (!cases || n <= 0 || !results) return IFC_BAD_ARGUMENT;
     const int prec = cases[0].precision;
     for (int c = 0; c < n; ++c) {

@@ -4,10 +4,19 @@
 #include <cstring>
 #include <new>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "ifc.h"
 #include "ifc_engine.cuh"
 
 using ifc::EngineBase;
+
+// NVTX range around a C ABI call, so timeline profilers show the library's
+// stages (solve, iterate, adjoint, VTK output) by name.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 struct ifc_solver {
     ifc_config cfg;
@@ -184,6 +193,7 @@ int ifc_device_ptr(ifc_solver *h, int field, void **dptr)
 
 int ifc_solve(ifc_solver *h, ifc_stats *stats)
 {
+    NvtxRange r("ifc_solve");
     IFC_GUARD(h)
     return h->eng->run(h->cfg.num_outer_iter, 1, stats);
     IFC_END(h)
@@ -191,6 +201,7 @@ int ifc_solve(ifc_solver *h, ifc_stats *stats)
 
 int ifc_iterate(ifc_solver *h, int n_outer, ifc_stats *stats)
 {
+    NvtxRange r("ifc_iterate");
     IFC_GUARD(h)
     return h->eng->run(n_outer, 0, stats);
     IFC_END(h)
@@ -227,6 +238,7 @@ int ifc_set_inlet_profile(ifc_solver *h, const double *profile)
 int ifc_adjoint(ifc_solver *h, int objective, const double *dJ_du, const double *dJ_dv, const double *dJ_dp,
                 int max_iter, double tol, double *dJ_dtheta, ifc_adjoint_result *result)
 {
+    NvtxRange nr("ifc_adjoint");
     if (objective != IFC_OBJ_PRESSURE_DROP && objective != IFC_OBJ_CUSTOM) return IFC_BAD_ARGUMENT;
     if (max_iter < 1 || !(tol >= 0.0)) return IFC_BAD_ARGUMENT;
     IFC_GUARD(h)
@@ -279,6 +291,7 @@ int ifc_get_stats(ifc_solver *h, ifc_stats *stats)
 
 int ifc_write_vtk(ifc_solver *h, const char *path)
 {
+    NvtxRange r("ifc_write_vtk");
     if (!path) return IFC_BAD_ARGUMENT;
     IFC_GUARD(h)
     const size_t bytes = h->eng->field_size(IFC_FIELD_U);

@@ -9,6 +9,10 @@ machine after `python oracle/build_ref.py` has compiled oracle/_ref/).
 * ref_solve_<case>.npz: u, v, p of the reference's Solver::solve() after a
   fixed number of outer iterations well past convergence, read back from its
   VTK output (6 significant digits).
+* oracle_cavity3d16.npz (--oracle-only needs no GPU): the 16^3 lid-driven
+  cavity solved by the FP64 oracle (red-black Gauss-Seidel, per-field rule
+  1e-5).  The reference's 3D build cannot run (it launches 2048-thread blocks
+  and indexes out of bounds), so this is the 3D pin.
 Copy the files into tests/golden/ to update the fixtures.
 """
 from __future__ import annotations
@@ -68,17 +72,36 @@ def run_solve_case(name: str, n_cells: int, out: str):
     np.savez_compressed(os.path.join(out, f"ref_solve_{name}.npz"), u=u, v=v, p=p, log=np.array(r.stdout[-2000:]))
 
 
+def oracle_cavity3d(out: str):
+    import ifc
+    import oracle as O
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import to_oracle_cfg
+
+    cfg = ifc.cavity3d(16)
+    o = O.Oracle(to_oracle_cfg(cfg), "d")
+    n, nm = o.solve()
+    f = {k: o.field(k).astype(np.float64).copy() for k in ("u", "v", "w", "p")}
+    np.savez_compressed(os.path.join(out, "oracle_cavity3d16.npz"), **f, iterations=np.array(n),
+                        converged=np.array(nm["converged"]))
+
+
 def main():
     import build_ref
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
+    ap.add_argument("--oracle-only", action="store_true")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
+    oracle_cavity3d(a.out)
+    if a.oracle_only:
+        return
     for name, cfg in build_ref.kernel_cases().items():
         run_kernel_case(name, cfg, a.out)
     for name, (cfg, *_rest) in build_ref.cases().items():
-        if name.startswith("channel512"):
+        if name.startswith("channel512") or name.endswith("_converge"):
             continue
         run_solve_case(name, cfg["nx"] * cfg["ny"], a.out)
     print("golden fixtures written to", a.out)

@@ -125,3 +125,17 @@ def test_oracle_converged_matches_reference_solve(name, closed, mode):
     if closed:
         p, pr = p - p.mean(), pr - pr.mean()
     assert rel_l2(p, pr) < 1e-5, rel_l2(p, pr)
+
+
+def test_oracle_3d_matches_fp64_golden():
+    """The 3D pin: the reference's own 3D build cannot run, so the 16^3
+    cavity solved by the FP64 oracle (red-black, per-field rule) is committed
+    as a fixture; the oracle must reproduce it (it is deterministic)."""
+    import ifc
+
+    g = fixture("oracle_cavity3d16.npz")
+    o = O.Oracle(to_oracle_cfg(ifc.cavity3d(16)), "d")
+    n, nm = o.solve()
+    assert n == int(g["iterations"]) and nm["converged"] == int(g["converged"])
+    for k in ("u", "v", "w", "p"):
+        assert rel_l2(o.field(k), g[k]) < 1e-12, k

@@ -146,3 +146,19 @@ def test_fused_graph_path_with_more_tiles_than_resident_ctas(gpu_ok, sweeps_per_
     o.solve(2)
     for k in ("u", "v", "p", "uf", "vf"):
         assert_bitwise(s.get(k), o.field(k), k)
+
+
+def test_device_3d_matches_fp64_golden(gpu_ok):
+    """FP32 device solve of the 16^3 cavity against the committed FP64-oracle
+    fixture (the 3D pin): relative L2 1e-4, p after removing its mean."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_cavity3d16.npz"))
+    s = ifc.Solver(ifc.cavity3d(16))
+    st = s.solve()
+    assert st["converged"]
+    for k in ("u", "v", "w", "p"):
+        a, b = s.get(k).astype(np.float64), g[k]
+        if k == "p":
+            a, b = a - a.mean(), b - b.mean()
+        assert rel_l2(a, b) < 1e-4, (k, rel_l2(a, b))
