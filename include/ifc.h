@@ -72,13 +72,13 @@ typedef struct ifc_config {
     int dim;                          /* 2 or 3 */
     int nx, ny, nz;                   /* nz is forced to 1 when dim == 2 */
     double xmin, xmax, ymin, ymax, zmin, zmax;
-    double thermal_conductivity;      /* carried for the VTK/config surface; the */
-    double specific_heat_capacity;    /* energy equation is not solved (as in the reference) */
+    double thermal_conductivity;      /* energy equation (ifc_solve_energy): Gamma = */
+    double specific_heat_capacity;    /* thermal_conductivity / specific_heat_capacity */
     double density;
     double dynamic_viscosity;
     int vel_bc_type[6];               /* velBCs::type, face order E W N S T B */
     double vel_bc_val[6][3];          /* velBCs::val[face][u,v,w] */
-    int temp_bc_type[6];              /* TempBCs (carried, unused) */
+    int temp_bc_type[6];              /* TempBCs: 0 Dirichlet (temp_bc_val), 1 Neumann (zero gradient) */
     double temp_bc_val[6];
     int num_outer_iter;
     int n_iter_u, n_iter_v, n_iter_w, n_iter_p;
@@ -192,6 +192,29 @@ int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result *results, v
  * has no profile.  No counterpart in the reference (its inlet is a compiled-in
  * constant); it lets a design loop update theta without rebuilding a handle. */
 int ifc_set_inlet_profile(ifc_solver *h, const double *profile);
+
+/* ---- energy equation on the converged flow ---- */
+typedef struct ifc_energy_result {
+    int status;
+    int sweeps;                       /* red-black sweeps done */
+    int converged;
+    double residual;                  /* last sweep's RMS change over the largest of this solve */
+    double device_ms;
+} ifc_energy_result;
+
+/* Steady temperature on the handle's current face mass fluxes (solve the
+ * flow first): div(rho u T) = div(Gamma grad T) with Gamma =
+ * thermal_conductivity / specific_heat_capacity, discretised like the
+ * momentum equations (upwind convection, central diffusion, the same
+ * boundary fold-in: wall form for Dirichlet faces, zero-gradient form for
+ * Neumann faces, temp_bc_type/temp_bc_val), solved by unrelaxed red-black
+ * Gauss-Seidel sweeps from the current temperature until the RMS change of
+ * a sweep falls below tol times the largest of this solve (FP64 norms), or
+ * max_sweeps (tol 0: exactly max_sweeps).  The result is the T field
+ * (IFC_FIELD_T, written by ifc_write_vtk).  Returns IFC_NOT_CONVERGED when
+ * max_sweeps ran out first.  The reference carries TempBCs and writes T but
+ * never solves the energy equation. */
+int ifc_solve_energy(ifc_solver *h, int max_sweeps, double tol, ifc_energy_result *result);
 
 /* ---- differentiation form: discrete adjoint of the converged 2D solve ---- */
 /* Objectives of ifc_adjoint. */

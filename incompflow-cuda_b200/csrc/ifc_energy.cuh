@@ -1,0 +1,84 @@
+// ifc_energy.cuh -- steady temperature transport on the converged flow.
+//
+// The reference allocates the temperature, carries its boundary conditions
+// (TempBCs, include/config.h:45-63) and thermal properties
+// (include/config.h:19-23) and writes it to VTK, but never solves for it.
+// Here the steady energy equation
+//     div(rho u T) = div(Gamma grad T),   Gamma = thermalConductivity / specificHeatCapacity
+// (so Gamma / rho is the reference's thermalDiffusivity) is discretised on the
+// converged face mass fluxes exactly as the momentum equations are: first-order
+// upwind convection and central diffusion links (kernels.cuh:97-134 with Gamma
+// in place of mu), and the boundary fold-in of kernels.cuh:252-334 -- the
+// wall/inlet form for a Dirichlet face (type 0, the given temperature) and
+// the zero-gradient form for a Neumann face (type 1).  The linear system is
+// solved with the library's red-black Gauss-Seidel sweep kernel, unrelaxed.
+#pragma once
+
+#include "ifc_kernels.cuh"
+
+namespace ifc {
+
+template <typename T>
+struct TempArgs {
+    T Dx, Dy, Dz;  // Gamma * A / d per direction, evaluated in the scalar type
+    int type[6];   // 0 Dirichlet, 1 Neumann (zero gradient)
+    T val[6];
+};
+
+template <typename T, int DIM>
+__device__ __forceinline__ void temp_fold(const Params<T> &P, const TempArgs<T> &ta, int face, int ex, int in,
+                                          T (&a)[7], T &b)
+{
+    const T e = a[ex];
+    if (ta.type[face] != 0) {
+        a[AC] = a[AC] + e;
+        a[ex] = (T)0;
+        return;
+    }
+    a[AC] = a[AC] - (T)2 * e;
+    a[in] = a[in] + e / (T)3;
+    b = b - P.d.c83 * e * ta.val[face];
+    a[ex] = (T)0;
+}
+
+// Coefficient planes (2*DIM+1, coef[cell + N*slot]) and source of the energy
+// equation of every cell.
+template <typename T, int DIM>
+__global__ void k_temp_assemble(Params<T> P, Fields<T> f, TempArgs<T> ta, T *coef, T *src)
+{
+    const Geo<T> &g = P.g;
+    const int N = g.N, nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) {
+        const int i = c % nx, j = (c / nx) % ny, k = c / pl;
+        const int fu = i + (nx + 1) * (j + ny * k), fv = i + nx * (j + (ny + 1) * k);
+        const T ue = f.uf[fu + 1], uw = f.uf[fu], vn = f.vf[fv + nx], vs = f.vf[fv];
+        T a[7];
+        a[AE] = g.rho * min0(ue) * g.Ax - ta.Dx;
+        a[AW] = g.rho * min0(-uw) * g.Ax - ta.Dx;
+        a[AN] = g.rho * min0(vn) * g.Ay - ta.Dy;
+        a[AS] = g.rho * min0(-vs) * g.Ay - ta.Dy;
+        a[AC] = -(a[AE] + a[AW] + a[AN] + a[AS]);
+        a[AT] = (T)0;
+        a[AB] = (T)0;
+        if (DIM == 3) {
+            const T wt = f.wf[c + pl], wb = f.wf[c];
+            a[AT] = g.rho * min0(wt) * g.Az - ta.Dz;
+            a[AB] = g.rho * min0(-wb) * g.Az - ta.Dz;
+            a[AC] += -(a[AT] + a[AB]);
+        }
+        T b = (T)0;
+        if (i == nx - 1) temp_fold<T, DIM>(P, ta, EAST, AE, AW, a, b);
+        if (i == 0) temp_fold<T, DIM>(P, ta, WEST, AW, AE, a, b);
+        if (j == ny - 1) temp_fold<T, DIM>(P, ta, NORTH, AN, AS, a, b);
+        if (j == 0) temp_fold<T, DIM>(P, ta, SOUTH, AS, AN, a, b);
+        if (DIM == 3) {
+            if (k == nz - 1) temp_fold<T, DIM>(P, ta, TOP, AT, AB, a, b);
+            if (k == 0) temp_fold<T, DIM>(P, ta, BOTTOM, AB, AT, a, b);
+        }
+#pragma unroll
+        for (int s = 0; s < 2 * DIM + 1; ++s) coef[c + (size_t)N * s] = a[s];
+        src[c] = b;
+    }
+}
+
+}  // namespace ifc

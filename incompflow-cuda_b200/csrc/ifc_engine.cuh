@@ -4,6 +4,7 @@
 // transfers.  Replaces the reference's Solver members (src/Solver.cu:13-966).
 #pragma once
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -16,6 +17,7 @@
 #include "ifc_kernels.cuh"
 #include "ifc_persist2d.cuh"
 #include "ifc_fused3d.cuh"
+#include "ifc_energy.cuh"
 
 namespace ifc {
 
@@ -33,6 +35,7 @@ struct EngineBase {
     virtual int time_stage(int stage, int reps, double *ms, int *launches) = 0;
     virtual int adjoint(const AdjointReq &rq, ifc_adjoint_result *res) = 0;
     virtual int set_inlet(const double *profile) = 0;
+    virtual int solve_energy(int max_sweeps, double tol, ifc_energy_result *res) = 0;
     std::string err;
 };
 
@@ -780,6 +783,79 @@ struct Engine : EngineBase {
             if (sq) sq[s] = ctl_h.last_sweep_sq[eq];
         }
         return IFC_OK;
+    }
+
+    // Steady temperature on the current flow (ifc_energy.cuh): assemble the
+    // energy equation once, then red-black sweeps of the temperature in chunks
+    // until the inner rule (RMS change of a sweep over the largest RMS change
+    // of this solve < tol) or max_sweeps.  The sweep bookkeeping uses the w
+    // slots of the control block, which the next outer iteration resets.
+    int solve_energy(int max_sweeps, double tol, ifc_energy_result *res) override
+    {
+        if (max_sweeps < 0 || !(tol >= 0.0)) {
+            err = "solve_energy: bad sweep count or tolerance";
+            return IFC_BAD_ARGUMENT;
+        }
+        const Geo<T> &g = P.g;
+        TempArgs<T> ta;
+        const T gam = (T)cfg.thermal_conductivity / (T)cfg.specific_heat_capacity;
+        ta.Dx = gam * g.Ax / g.dx;
+        ta.Dy = gam * g.Ay / g.dy;
+        ta.Dz = gam * g.Az / g.dz;
+        for (int q = 0; q < 6; ++q) {
+            ta.type[q] = cfg.temp_bc_type[q];
+            ta.val[q] = (T)cfg.temp_bc_val[q];
+        }
+        Params<T> PT = P;
+        PT.g.relax[EQ_W] = (T)1;
+        PT.g.tol[EQ_W] = tol;
+        const long long N = g.N;
+        T *src = f.tmp;
+        IFC_CK(cudaStreamSynchronize(stream));
+        IFC_CK(cudaEventRecord(ev0, stream));
+        if (dim == 2) k_temp_assemble<T, 2><<<grid(N), 256, 0, stream>>>(P, f, ta, f.mc, src);
+        else k_temp_assemble<T, 3><<<grid(N), 256, 0, stream>>>(P, f, ta, f.mc, src);
+        k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << EQ_W);
+        SweepArgs<T, 1> A;
+        A.coef = f.mc;
+        A.phi[0] = f.temp;
+        A.old[0] = f.temp;
+        A.src[0] = src;
+        A.eq[0] = EQ_W;
+        A.active[0] = 1;
+        const long long half = (long long)((g.nx + 1) / 2) * g.ny * g.nz;
+        int done = 0;
+        while (done < max_sweeps) {
+            const int chunk = max_sweeps - done < 25 ? max_sweeps - done : 25;
+            for (int q = 0; q < chunk; ++q)
+                for (int color = 0; color < 2; ++color) {
+                    A.color = color;
+                    if (dim == 2) k_sweep<T, 2, 1><<<grid(half), 256, 0, stream>>>(PT, A, ctl, partials);
+                    else k_sweep<T, 3, 1><<<grid(half), 256, 0, stream>>>(PT, A, ctl, partials);
+                }
+            done += chunk;
+            IFC_CK(cudaGetLastError());
+            int rc = read_ctl();
+            if (rc != IFC_OK) return rc;
+            if (ctl_h.stop[EQ_W]) break;
+        }
+        IFC_CK(cudaEventRecord(ev1, stream));
+        int rc = read_ctl();
+        if (rc != IFC_OK) return rc;
+        float ms = 0.f;
+        IFC_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        if (res) {
+            std::memset(res, 0, sizeof(*res));
+            res->sweeps = ctl_h.sweeps[EQ_W];
+            res->converged = ctl_h.stop[EQ_W];
+            const double last = std::sqrt(ctl_h.last_sweep_sq[EQ_W] / (double)N);
+            res->residual = ctl_h.inner_max[EQ_W] > 0.0 ? last / ctl_h.inner_max[EQ_W] : 0.0;
+            res->device_ms = ms;
+            res->status = ctl_h.stop[EQ_W] || tol == 0.0 ? IFC_OK : IFC_NOT_CONVERGED;
+        }
+        k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << EQ_W);
+        IFC_CK(cudaStreamSynchronize(stream));
+        return ctl_h.stop[EQ_W] || tol == 0.0 ? IFC_OK : IFC_NOT_CONVERGED;
     }
 
     int set_inlet(const double *profile) override

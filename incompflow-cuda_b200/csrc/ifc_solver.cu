@@ -228,6 +228,17 @@ int ifc_time_stage(ifc_solver *h, int stage, int reps, double *ms, int *launches
     IFC_END(h)
 }
 
+int ifc_solve_energy(ifc_solver *h, int max_sweeps, double tol, ifc_energy_result *result)
+{
+    NvtxRange r("ifc_solve_energy");
+    IFC_GUARD(h)
+    ifc_energy_result tmp;
+    const int rc = h->eng->solve_energy(max_sweeps, tol, result ? result : &tmp);
+    if (result) result->status = rc;
+    return rc;
+    IFC_END(h)
+}
+
 int ifc_set_inlet_profile(ifc_solver *h, const double *profile)
 {
     IFC_GUARD(h)

@@ -87,6 +87,14 @@ class IfcAdjointResult(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class IfcEnergyResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("sweeps", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
+                ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 OBJ_PRESSURE_DROP, OBJ_CUSTOM = 0, 1
 _DP = C.POINTER(C.c_double)
 
@@ -117,6 +125,7 @@ EXPORTS = {
                               C.POINTER(IfcAdjointResult)]),
     "ifc_adjoint_apply": (C.c_int, [C.c_void_p] + [_DP] * 12),
     "ifc_set_inlet_profile": (C.c_int, [C.c_void_p, _DP]),
+    "ifc_solve_energy": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(IfcEnergyResult)]),
 }
 
 
@@ -216,6 +225,10 @@ def make_struct(cfg: dict) -> tuple[IfcConfig, object]:
         setattr(c, k, float(cfg[k]))
     c.thermal_conductivity = float(cfg.get("thermalConductivity", 1.0))
     c.specific_heat_capacity = float(cfg.get("specificHeatCapacity", 1.0))
+    if "TempBC_type" in cfg:
+        for f in range(6):
+            c.temp_bc_type[f] = int(cfg["TempBC_type"][f])
+            c.temp_bc_val[f] = float(cfg["TempBC_val"][f])
     c.density = float(cfg["density"])
     c.dynamic_viscosity = float(cfg["dynamicViscosity"])
     for f in range(6):
@@ -333,6 +346,13 @@ class Solver:
 
     def write_vtk(self, path: str):
         self._check(load().ifc_write_vtk(self._h, path.encode()), "write_vtk")
+
+    def solve_energy(self, max_sweeps: int = 20000, tol: float = 1e-6) -> dict:
+        """Steady temperature on the current flow (ifc_solve_energy)."""
+        r = IfcEnergyResult()
+        self._check(load().ifc_solve_energy(self._h, int(max_sweeps), float(tol), C.byref(r)), "solve_energy",
+                    allow=(OK, NOT_CONVERGED))
+        return r.as_dict()
 
     def set_inlet_profile(self, profile):
         a = np.ascontiguousarray(profile, dtype=np.float64)

@@ -265,3 +265,103 @@ class AdjointOracle(Oracle):
                 break
         out, lth, lmu = self.apply_transpose(lam)
         return lth, lmu, it
+
+
+# ---------------------------------------------------------------- energy
+# The reference never solves its temperature; the library's energy equation
+# (incompflow-cuda_b200/csrc/ifc_energy.cuh) discretises div(rho u T) =
+# div(Gamma grad T), Gamma = k / cp, like the reference's momentum equations
+# (include/kernels.cuh:97-134 with Gamma for mu, boundary fold-in of
+# :252-334: wall form on Dirichlet faces, zero-gradient form on Neumann
+# faces).  These functions restate it in numpy, operation by operation in the
+# scalar type, as the checker of the device solve.
+
+def _min0(x):
+    return np.where(x < 0, x, x.dtype.type(0))
+
+
+def energy_assemble(cfg: dict, uf, vf, wf, prec: str = "f"):
+    """Coefficient planes (2*dim+1, slot-major as the library's) and source of
+    the energy equation on the given face velocities."""
+    T = np.float32 if prec == "f" else np.float64
+    dim, nx, ny = cfg["dim"], cfg["nx"], cfg["ny"]
+    nz = cfg.get("nz", 1) if dim == 3 else 1
+    dx = (T(cfg["xmax"]) - T(cfg["xmin"])) / T(nx)
+    dy = (T(cfg["ymax"]) - T(cfg["ymin"])) / T(ny)
+    dz = (T(cfg["zmax"]) - T(cfg["zmin"])) / T(nz)
+    Ax, Ay, Az = dy * dz, dz * dx, dx * dy
+    rho = T(cfg["density"])
+    gam = T(cfg.get("thermalConductivity", 1.0)) / T(cfg.get("specificHeatCapacity", 1.0))
+    Dx, Dy, Dz = gam * Ax / dx, gam * Ay / dy, gam * Az / dz
+    uf = np.asarray(uf, T).reshape(nz, ny, nx + 1)
+    vf = np.asarray(vf, T).reshape(nz, ny + 1, nx)
+    a = {}
+    a["E"] = rho * _min0(uf[:, :, 1:]) * Ax - Dx
+    a["W"] = rho * _min0(-uf[:, :, :-1]) * Ax - Dx
+    a["N"] = rho * _min0(vf[:, 1:, :]) * Ay - Dy
+    a["S"] = rho * _min0(-vf[:, :-1, :]) * Ay - Dy
+    a["C"] = -(((a["E"] + a["W"]) + a["N"]) + a["S"])
+    a["T"] = np.zeros_like(a["C"])
+    a["B"] = np.zeros_like(a["C"])
+    if dim == 3:
+        wf = np.asarray(wf, T).reshape(nz + 1, ny, nx)
+        a["T"] = rho * _min0(wf[1:]) * Az - Dz
+        a["B"] = rho * _min0(-wf[:-1]) * Az - Dz
+        a["C"] = a["C"] + (-(a["T"] + a["B"]))
+    b = np.zeros_like(a["C"])
+    c83 = T(8) / T(3)
+    faces = [(0, "E", "W", (slice(None), slice(None), -1)), (1, "W", "E", (slice(None), slice(None), 0)),
+             (2, "N", "S", (slice(None), -1, slice(None))), (3, "S", "N", (slice(None), 0, slice(None)))]
+    if dim == 3:
+        faces += [(4, "T", "B", (-1, slice(None), slice(None))), (5, "B", "T", (0, slice(None), slice(None)))]
+    types = cfg.get("TempBC_type", [1, 1, 0, 0, 1, 1])
+    vals = cfg.get("TempBC_val", [0.0, 0.0, 293.0, 373.0, 0.0, 0.0])
+    for f, ex, inn, sl in faces:
+        e = a[ex][sl].copy()
+        if types[f] != 0:
+            a["C"][sl] = a["C"][sl] + e
+        else:
+            a["C"][sl] = a["C"][sl] - T(2) * e
+            a[inn][sl] = a[inn][sl] + e / T(3)
+            b[sl] = b[sl] - c83 * e * T(vals[f])
+        a[ex][sl] = T(0)
+    order = ["C", "E", "W", "N", "S"] + (["T", "B"] if dim == 3 else [])
+    return np.stack([a[k] for k in order]), b
+
+
+def energy_sweeps(cfg: dict, coef, src, temp, n: int, prec: str = "f"):
+    """n unrelaxed red-black Gauss-Seidel sweeps of the temperature (colour 0
+    then colour 1, the library's point update); returns T and the FP64 sum of
+    squared changes of each sweep."""
+    Tt = np.float32 if prec == "f" else np.float64
+    dim = cfg["dim"]
+    nx, ny = cfg["nx"], cfg["ny"]
+    nz = cfg.get("nz", 1) if dim == 3 else 1
+    coef = np.asarray(coef, Tt)
+    a = {k: coef[s].reshape(nz, ny, nx) for s, k in enumerate(["C", "E", "W", "N", "S", "T", "B"][: coef.shape[0]])}
+    src = np.asarray(src, Tt).reshape(nz, ny, nx)
+    t = np.asarray(temp, Tt).reshape(nz, ny, nx).copy()
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    colour = (i + j + k) & 1
+    zero = Tt(0)
+    sums = []
+    for _ in range(n):
+        sq = 0.0
+        for c in (0, 1):
+            pE = np.zeros_like(t); pE[:, :, :-1] = t[:, :, 1:]
+            pW = np.zeros_like(t); pW[:, :, 1:] = t[:, :, :-1]
+            pN = np.zeros_like(t); pN[:, :-1, :] = t[:, 1:, :]
+            pS = np.zeros_like(t); pS[:, 1:, :] = t[:, :-1, :]
+            npv = src - a["E"] * pE - a["W"] * pW - a["N"] * pN - a["S"] * pS
+            if dim == 3:
+                pT = np.zeros_like(t); pT[:-1] = t[1:]
+                pB = np.zeros_like(t); pB[1:] = t[:-1]
+                npv = npv - (a["T"] * pT + a["B"] * pB)
+            npv = npv / a["C"]
+            d = Tt(1) * (npv - t)
+            new = t + d
+            m = colour == c
+            t = np.where(m, new, t)
+            sq += float(np.sum(np.where(m, d, zero).astype(np.float64) ** 2))
+        sums.append(sq)
+    return t.ravel(), sums
