@@ -215,6 +215,15 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
     for (int c = 0; c < 2; ++c)
 #pragma unroll
         for (int k = 0; k < CPT; ++k) dq[c][k] = tile_distance<W, H, TX, TY>(cq[c][k]);
+    // Warps none of whose cells lie in the tile contribute only zeros to the
+    // per-sweep sums; they skip the shuffle reduction (the shuffle unit is
+    // shared by the whole SM) and report 0.0, the value the reduction gives.
+    bool mine = false;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) mine |= dq[c][k] == 0;
+    const bool wsum = __any_sync(0xffffffffu, mine);
     __syncthreads();
 
     const int npass_m = (max(pa.n_iter[0], pa.n_iter[1]) + KS - 1) / KS;
@@ -257,6 +266,8 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 s2[q] = in ? f.p[id] : (T)0;
             }
             __syncthreads();
+            // The sums of a phase's last pass are never reduced.
+            const bool last = pass >= npass_m - 1;
             T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cbu[2][CPT], cbv[2][CPT];
             bool own[2][CPT];
 #pragma unroll
@@ -309,21 +320,25 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                         if (du && dq[color][k] <= 2 * ns[0] - 1 - hs) {
                             s0[q] = point_update<T, 2>(a7, cbu[color][k], s0[q], s0[q + 1], s0[q - 1], s0[q + W],
                                                        s0[q - W], (T)0, (T)0, ru, d);
-                            if (own[color][k]) su += (double)d * (double)d;
+                            if (!last && own[color][k]) su += (double)d * (double)d;
                         }
                         if (dv && dq[color][k] <= 2 * ns[1] - 1 - hs) {
                             s1[q] = point_update<T, 2>(a7, cbv[color][k], s1[q], s1[q + 1], s1[q - 1], s1[q + W],
                                                        s1[q - W], (T)0, (T)0, rv, d);
-                            if (own[color][k]) sv += (double)d * (double)d;
+                            if (!last && own[color][k]) sv += (double)d * (double)d;
                         }
                     }
                     __syncthreads();
                 }
-                su = warp_sum(su);
-                sv = warp_sum(sv);
-                if ((tid & 31) == 0) {
-                    wred[tid >> 5][s] = su;
-                    wred[tid >> 5][KS + s] = sv;
+                if (!last) {
+                    if (wsum) {
+                        su = warp_sum(su);
+                        sv = warp_sum(sv);
+                    }
+                    if ((tid & 31) == 0) {
+                        wred[tid >> 5][s] = su;
+                        wred[tid >> 5][KS + s] = sv;
+                    }
                 }
             }
             for (int q = tid; q < TX * TY; q += NT) {
@@ -335,7 +350,6 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 bv[mcur ^ 1][id] = s1[b * W + a];
             }
             mcur ^= 1;
-            const bool last = pass >= npass_m - 1;
             if (!last) block_partials<2 * KS, 2 * KS, NT>(&wred[0][0], partials, G);
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
             if (!last) reduce_partials<2 * KS, NT>(partials, G, tot);
@@ -392,6 +406,7 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 s1[q] = in ? (T)1 / f.ac[id] : (T)0;
             }
             __syncthreads();
+            const bool last = pass == npass_p - 1;
             T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cb[2][CPT];
             bool own[2][CPT];
 #pragma unroll
@@ -434,12 +449,14 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                         T d;
                         s0[q] = point_update<T, 2>(a7, cb[color][k], s0[q], s0[q + 1], s0[q - 1], s0[q + W],
                                                    s0[q - W], (T)0, (T)0, relax, d);
-                        if (own[color][k]) sx += (double)d * (double)d;
+                        if (!last && own[color][k]) sx += (double)d * (double)d;
                     }
                     __syncthreads();
                 }
-                sx = warp_sum(sx);
-                if ((tid & 31) == 0) wred[tid >> 5][s] = sx;
+                if (!last) {
+                    if (wsum) sx = warp_sum(sx);
+                    if ((tid & 31) == 0) wred[tid >> 5][s] = sx;
+                }
             }
             for (int q = tid; q < TX * TY; q += NT) {
                 const int a = H + q % TX, b = H + q / TX;
@@ -448,7 +465,6 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                 bp[pcur ^ 1][gi + nx * gj] = s0[b * W + a];
             }
             pcur ^= 1;
-            const bool last = pass == npass_p - 1;
             if (!last) block_partials<KS, 2 * KS, NT>(&wred[0][0], partials, G);
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
             if (!last) reduce_partials<KS, NT>(partials, G, tot);
