@@ -63,13 +63,24 @@ def parse():
     ap.add_argument("--n3d", type=int, default=128, help="precision form: cells per direction")
     ap.add_argument("--max-outer", type=int, default=8000, help="precision form: outer-iteration cap")
     ap.add_argument("--cases", type=int, default=256, help="batch form: cases")
+    ap.add_argument("--convection", default="upwind",
+                    choices=["upwind", "central", "sou", "quick", "minmod", "van_leer"],
+                    help="plain form: convection scheme (upwind is the reference's; the others run by "
+                         "deferred correction)")
     return ap.parse_args()
+
+
+CONVECTION = "upwind"
 
 
 def workload_cfg():
     import ifc
 
-    return ifc.channel2d(512, 128)
+    return ifc.channel2d(512, 128, convection_scheme=CONVECTION)
+
+
+def workload_name():
+    return WORKLOAD if CONVECTION == "upwind" else f"{WORKLOAD}_{CONVECTION}"
 
 
 def measured_peaks():
@@ -179,7 +190,7 @@ def cpu_baseline(seconds: float):
         updates += o.N * (nm["sweeps"][0] + nm["sweeps"][1] + nm["sweeps"][3])
     dt = time.perf_counter() - t0
     return {"value": updates / dt, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": f"{its} outer iterations of {WORKLOAD} from rest, serial C oracle (FP32, red-black GS, "
+            "sample": f"{its} outer iterations of {workload_name()} from rest, serial C oracle (FP32, red-black GS, "
                       f"gcc -O2), {dt:.1f} s on one core of {host_cpu()}"}
 
 
@@ -293,7 +304,8 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic: flow from rest, advanced by the warm-up steps",
-            "config": {"workload": WORKLOAD, "nx": 512, "ny": 128, "outer_iterations_per_step": OUTER_PER_STEP,
+            "config": {"workload": workload_name(), "nx": 512, "ny": 128,
+                       "outer_iterations_per_step": OUTER_PER_STEP, "convection": CONVECTION,
                        "sweeps_u_v_p": [cfg["nIter_u"], cfg["nIter_v"], cfg["nIter_p"]],
                        "linear_solver": "red-black Gauss-Seidel", "precision": "fp32 sweeps, fp64 norms",
                        "l2": "flushed (256 MB write) between timed steps",
@@ -498,7 +510,7 @@ def run_precision(args):
         return
     torch.cuda.set_device(local)
     n = args.n3d
-    cfg = ifc.cavity3d(n, re=400.0, numOuterIter=args.max_outer)
+    cfg = ifc.cavity3d(n, re=400.0, numOuterIter=args.max_outer, convection_scheme=CONVECTION)
     clocks = ClockSampler(local)
     clocks.start()
     s32 = ifc.Solver(dict(cfg, precision="f", criterion=ifc.CRIT_REFERENCE))
@@ -540,8 +552,9 @@ def run_precision(args):
         "metric": "time to convergence", "value": st32["device_ms"] / 1e3, "unit": "s", "higher_is_better": False,
         "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": st32["device_ms"], "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 sweeps, f64 reductions", "data": "synthetic: flow from rest",
-        "config": {"workload": PREC_WORKLOAD, "n": n, "criterion": "reference rule (norms over the p-norm max), 1e-5",
-                   "max_outer": args.max_outer},
+        "config": {"workload": PREC_WORKLOAD if CONVECTION == "upwind" else f"{PREC_WORKLOAD}_{CONVECTION}", "n": n,
+                   "criterion": "reference rule (norms over the p-norm max), 1e-5",
+                   "max_outer": args.max_outer, "convection": CONVECTION},
         "fp32": {"converged": bool(st32["converged"]), "outer_iterations": k32,
                  "ms_per_outer_iteration": st32["device_ms"] / max(k32, 1),
                  "cell_updates_per_s": st32["cell_updates"] / (st32["device_ms"] * 1e-3)},
@@ -698,6 +711,10 @@ def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
         return
+    if CONVECTION != "upwind":
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference has first-order upwind convection only"}))
+        return
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_bench_channel512x128")
     if os.path.exists(ref_bin):
         out = subprocess.run([ref_bin, str(args.warmup), str(args.steps)], capture_output=True, text=True,
@@ -732,7 +749,9 @@ def run_reference(args):
 
 
 def main():
+    global CONVECTION
     args = parse()
+    CONVECTION = args.convection
     if args.impl == "reference":
         run_reference(args)
     elif args.form == "adjoint":

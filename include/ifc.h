@@ -50,6 +50,21 @@ enum { IFC_GAUSS_SEIDEL = 0, IFC_JACOBI = 1 };
  * PER_FIELD divides each norm by its own running max (FP64). */
 enum { IFC_CRIT_REFERENCE = 0, IFC_CRIT_PER_FIELD = 1 };
 
+/* Convection schemes of the momentum equations.  IFC_CONV_UPWIND is the
+ * reference's first-order upwind (include/kernels.cuh:97-134) and the default;
+ * the others are applied by deferred correction: the links stay upwind and
+ * F_f (phi_f,HO - phi_f,upwind) of every interior face whose far-upwind cell
+ * is inside the domain enters the source, lagged by one outer iteration.
+ * The reference lists such schemes as planned (README.md:412). */
+enum {
+    IFC_CONV_UPWIND = 0,
+    IFC_CONV_CENTRAL = 1,
+    IFC_CONV_SOU = 2,        /* second-order upwind (linear upwind) */
+    IFC_CONV_QUICK = 3,
+    IFC_CONV_MINMOD = 4,     /* TVD, minmod limiter */
+    IFC_CONV_VAN_LEER = 5    /* TVD, van Leer limiter */
+};
+
 /* Field ids for ifc_get_field / ifc_set_field / ifc_device_ptr.  Layouts follow
  * the reference: cells i + nx*(j + ny*k); uf i + (nx+1)*(j + ny*k);
  * vf i + nx*(j + (ny+1)*k); wf i + nx*(j + ny*k) with k in [0, nz].
@@ -93,6 +108,8 @@ typedef struct ifc_config {
     int log_level;                    /* 0 silent, 1 reference log cadence on stdout */
     const double *inlet_profile;      /* optional west-face inlet velocity per boundary cell (ny*nz) */
     void *stream;                     /* cudaStream_t to run on, or NULL for a private stream */
+    int convection_scheme;            /* IFC_CONV_* (default IFC_CONV_UPWIND); ifc_batch_solve and
+                                         ifc_adjoint take IFC_CONV_UPWIND only */
 } ifc_config;
 
 typedef struct ifc_stats {
@@ -244,8 +261,9 @@ typedef struct ifc_adjoint_result {
  * taken at the handle's current fields (solve first); all adjoint arithmetic
  * is FP64 for either precision of the handle.  dJ_du/dJ_dv/dJ_dp: host arrays
  * of nx*ny doubles (NULL = 0), read with IFC_OBJ_CUSTOM only.  dJ_dtheta:
- * host array of ny doubles (zeros unless the west face is an inlet).  2D and
- * red-black Gauss-Seidel only (IFC_UNSUPPORTED otherwise).  Returns
+ * host array of ny doubles (zeros unless the west face is an inlet).  2D,
+ * red-black Gauss-Seidel and upwind convection only (IFC_UNSUPPORTED
+ * otherwise).  Returns
  * IFC_NOT_CONVERGED when max_iter passes did not reach tol (the gradient of
  * the last iterate is still returned).  No counterpart in the reference. */
 int ifc_adjoint(ifc_solver *h, int objective, const double *dJ_du, const double *dJ_dv, const double *dJ_dp,
@@ -263,7 +281,8 @@ int ifc_adjoint_apply(ifc_solver *h, const double *lam_u, const double *lam_v, c
 /* ---- single steps, for testing one application of each device kernel ---- */
 enum {
     IFC_STAGE_FACE_BC = 0,       /* first iteration: face init; then face BCs (kernels.cuh:10-95) */
-    IFC_STAGE_MOM_ASSEMBLE = 1,  /* materialise coefficients + sources (kernels.cuh:97-334) */
+    IFC_STAGE_MOM_ASSEMBLE = 1,  /* materialise coefficients + sources (kernels.cuh:97-334), with the
+                                    deferred-correction sources when convection_scheme != UPWIND */
     IFC_STAGE_MOM_SOLVE = 2,     /* assembly fused with the u,v,w sweeps (kernels.cuh:926-1005) */
     IFC_STAGE_RHIE_CHOW = 3,     /* faces + face BCs + p' source + mass norm (kernels.cuh:336-500,542-581) */
     IFC_STAGE_PCORR_COEF = 4,    /* materialise p' link coefficients (kernels.cuh:502-540) */

@@ -308,8 +308,8 @@ template <typename T>
 int adjoint_run(AdjointCtx *&ctx, const ifc_config &cfg, Params<double> Pd, const Fields<T> &f, const T *inlet,
                 cudaStream_t stream, const AdjointReq &rq, ifc_adjoint_result *res, std::string &err)
 {
-    if (Pd.g.dim != 2 || cfg.linear_solver != IFC_GAUSS_SEIDEL) {
-        err = "the adjoint supports 2D red-black Gauss-Seidel solves only";
+    if (Pd.g.dim != 2 || cfg.linear_solver != IFC_GAUSS_SEIDEL || cfg.convection_scheme != IFC_CONV_UPWIND) {
+        err = "the adjoint supports 2D red-black Gauss-Seidel solves with upwind convection only";
         return IFC_UNSUPPORTED;
     }
     if (!ctx) {

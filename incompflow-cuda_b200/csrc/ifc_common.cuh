@@ -36,6 +36,7 @@ struct Geo {
     T bcv[6][3];
     const T *inlet;                 // west-face inlet profile (device, ny*nz) or nullptr
     int criterion;                  // 0 reference rule, 1 per-field rule
+    int conv;                       // convection scheme (ifc_convection.cuh); 0 upwind
 };
 
 template <typename T>
@@ -47,6 +48,7 @@ struct Fields {
     T *su, *sv, *sw, *sp;           // momentum sources and p' source (mass imbalance)
     T *tmp;                         // scratch copy for Jacobi sweeps (3*N)
     T *rac;                         // 1/aC (3D p' sweeps)
+    T *sdc;                         // deferred-correction sources of u, v, w (dim planes; conv != 0)
 };
 
 struct LogRec {

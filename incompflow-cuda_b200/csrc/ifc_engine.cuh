@@ -85,6 +85,7 @@ Params<T> make_params(const ifc_config &c)
     }
     g.inlet = nullptr;
     g.criterion = c.criterion == IFC_CRIT_REFERENCE ? 0 : 1;
+    g.conv = c.convection_scheme;
     Derived<T> &d = P.d;
     d.Dx = g.mu * g.Ax / g.dx;
     d.Dy = g.mu * g.Ay / g.dy;
@@ -197,6 +198,7 @@ struct Engine : EngineBase {
         A_(f.uf, nface(0)); A_(f.vf, nface(1)); A_(f.wf, nface(2));
         A_(f.ac, N); A_(f.mc, N * nc); A_(f.pcoef, N * nc);
         A_(f.su, N); A_(f.sv, N); A_(f.sw, N); A_(f.sp, N); A_(f.tmp, 3 * N); A_(f.rac, N);
+        if (c.convection_scheme != IFC_CONV_UPWIND) A_(f.sdc, (size_t)dim * N);
         // One FP64 partial per value and block: the grid-stride kernels use at
         // most max_grid blocks, the tiled 2D kernels one block per 32x8 tile.
         const size_t tiles = (size_t)((P.g.nx + 31) / 32) * (size_t)((P.g.ny + 7) / 8) * (size_t)P.g.nz;
@@ -436,6 +438,16 @@ struct Engine : EngineBase {
         }
     }
 
+    // Deferred-correction sources of the momentum equations (higher-order
+    // convection), from the fields at the start of the outer iteration.
+    template <int DIM>
+    void enq_dc_source()
+    {
+        if (P.g.conv == CONV_UPWIND) return;
+        k_dc_source<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f);
+        ++launches;
+    }
+
     template <int DIM>
     void enq_mom_assemble()
     {
@@ -544,6 +556,7 @@ struct Engine : EngineBase {
     {
         // The boundary faces of each iteration are written by the previous
         // iteration's update kernel; run() applies them before the first.
+        enq_dc_source<DIM>();
         enq_mom_solve<DIM>();
         enq_rhie_chow<DIM>();
         enq_pcorr_solve<DIM>();
@@ -722,9 +735,13 @@ struct Engine : EngineBase {
     {
         switch (stage) {
         case IFC_STAGE_FACE_BC: enq_face_bc<DIM>(); break;
-        case IFC_STAGE_MOM_ASSEMBLE: enq_mom_assemble<DIM>(); break;
+        case IFC_STAGE_MOM_ASSEMBLE:
+            enq_dc_source<DIM>();
+            enq_mom_assemble<DIM>();
+            break;
         case IFC_STAGE_MOM_SOLVE:
             k_reset_inner<<<1, 1, 0, stream>>>(ctl, 7);
+            enq_dc_source<DIM>();
             enq_mom_solve<DIM>();
             break;
         case IFC_STAGE_RHIE_CHOW: enq_rhie_chow<DIM>(); break;

@@ -156,6 +156,7 @@ __global__ void __launch_bounds__(NT) k_mom_pass2d(Params<T> P, Fields<T> f, Ctl
             T a7[7], b3[3];
             mom_cell<T, 2>(P, gi, gj, 0, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], (T)0, (T)0, sp[q],
                            sp[q - 1], sp[q + 1], sp[q - W], sp[q + W], (T)0, (T)0, a7, b3);
+            add_dc<T, 2>(P, f, gi + nx * gj, b3);
             cE[c][k] = a7[AE];
             cW[c][k] = a7[AW];
             cN[c][k] = a7[AN];

@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(256) k_mom_half3d(Params<T> P, Fields<T> f, Ct
                            i > 0 ? f.p[c - 1] : (T)0, i < nx - 1 ? f.p[c + 1] : (T)0, j > 0 ? f.p[c - nx] : (T)0,
                            j < ny - 1 ? f.p[c + nx] : (T)0, k > 0 ? f.p[c - pl] : (T)0, k < nz - 1 ? f.p[c + pl] : (T)0,
                            a, b);
+            add_dc<T, 3>(P, f, c, b);
             if (h.first) f.ac[c] = a[AC];
 #pragma unroll
             for (int m = 0; m < 3; ++m) {

@@ -8,6 +8,7 @@
 #pragma once
 
 #include "ifc_physics.cuh"
+#include "ifc_convection.cuh"
 
 namespace ifc {
 
@@ -110,6 +111,7 @@ __device__ __forceinline__ void mom_cell_global(const Params<T> &P, const Fields
     mom_cell<T, DIM>(P, i, j, k, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], wb, wt, f.p[c],
                      i > 0 ? f.p[c - 1] : (T)0, i < nx - 1 ? f.p[c + 1] : (T)0,
                      j > 0 ? f.p[c - nx] : (T)0, j < ny - 1 ? f.p[c + nx] : (T)0, pB, pT, a, b);
+    add_dc<T, DIM>(P, f, c, b);
 }
 
 // ---- momentum assembly (materialised) ------------------------------------

@@ -250,6 +250,20 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         // next barrier runs out and the launch ends with the timeout status.
         if (pa.stall_test && blockIdx.x == 0) { failed = true; break; }
 
+        // ---- deferred-correction sources (higher-order convection), from the
+        // fields at the start of the outer iteration; the momentum passes read
+        // them for their halos too, so a barrier follows ----
+        if (g.conv != CONV_UPWIND) {
+            for (int q = tid; q < TX * TY; q += NT) {
+                const int i = x0 + q % TX, j = y0 + q / TX;
+                if (i >= nx || j >= ny) continue;
+                const int c = i + nx * j;
+                f.sdc[c] = dc_cell<T, 2>(P, f, f.u, i, j, 0);
+                f.sdc[N + c] = dc_cell<T, 2>(P, f, f.v, i, j, 0);
+            }
+            if (!grid_sync(bar, G, epoch)) { failed = true; break; }
+        }
+
         // ---------------- momentum passes ----------------
         for (int pass = 0; pass < (npass_m > 0 ? npass_m : 1); ++pass) {
             int ns[2] = {clamp_sweeps(pa.n_iter[0], pass, KS), clamp_sweeps(pa.n_iter[1], pass, KS)};
@@ -285,6 +299,7 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                     T a7[7], b3[3];
                     mom_cell<T, 2>(P, gi, gj, 0, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], (T)0, (T)0, s2[q],
                                    s2[q - 1], s2[q + 1], s2[q - W], s2[q + W], (T)0, (T)0, a7, b3);
+                    add_dc<T, 2>(P, f, fv, b3);
                     cE[c][k] = a7[AE];
                     cW[c][k] = a7[AW];
                     cN[c][k] = a7[AN];

@@ -115,6 +115,18 @@ __device__ __forceinline__ void mom_cell(const Params<T> &P, int i, int j, int k
     }
 }
 
+// Adds the deferred-correction sources of cell c (higher-order convection,
+// ifc_convection.cuh) to the momentum sources b after the boundary fold-in.
+template <typename T, int DIM>
+__device__ __forceinline__ void add_dc(const Params<T> &P, const Fields<T> &f, int c, T (&b)[3])
+{
+    if (P.g.conv == 0) return;
+    const int N = P.g.N;
+    b[0] = b[0] + f.sdc[c];
+    b[1] = b[1] + f.sdc[N + c];
+    if (DIM == 3) b[2] = b[2] + f.sdc[2 * N + c];
+}
+
 // One relaxed point update, kernels.cuh:976-988: out-of-domain neighbours
 // enter as 0 (their links are 0 after the fold-in anyway).
 template <typename T, int DIM>

@@ -78,6 +78,7 @@ int ifc_config_default(ifc_config *c)
     c->log_level = 0;
     c->inlet_profile = nullptr;
     c->stream = nullptr;
+    c->convection_scheme = IFC_CONV_UPWIND;
     return IFC_OK;
 }
 
@@ -100,6 +101,7 @@ int ifc_config_check(const ifc_config *c)
     if (c->criterion != IFC_CRIT_REFERENCE && c->criterion != IFC_CRIT_PER_FIELD) return IFC_BAD_CONFIG;
     if (c->pin_pressure < -1 || c->pin_pressure > 1) return IFC_BAD_CONFIG;
     if (c->sweeps_per_pass < 0 || c->sweeps_per_pass > 16) return IFC_BAD_CONFIG;
+    if (c->convection_scheme < IFC_CONV_UPWIND || c->convection_scheme > IFC_CONV_VAN_LEER) return IFC_BAD_CONFIG;
     return IFC_OK;
 }
 

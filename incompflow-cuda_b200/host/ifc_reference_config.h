@@ -14,6 +14,12 @@
 #define IFC_SOLVER_CRITERION IFC_CRIT_REFERENCE
 #endif
 
+#ifndef IFC_SOLVER_CONVECTION
+// First-order upwind, the reference's only convection scheme, unless the
+// including program selects another IFC_CONV_* value.
+#define IFC_SOLVER_CONVECTION IFC_CONV_UPWIND
+#endif
+
 inline ifc_config ifc_config_from_reference()
 {
     ifc_config c;
@@ -39,6 +45,7 @@ inline ifc_config ifc_config_from_reference()
     c.tol_u = tol_u; c.tol_v = tol_v; c.tol_w = tol_w; c.tol_p = tol_p; c.tol_mass = tol_mass;
     c.precision = sizeof(scalar) == sizeof(double) ? IFC_FP64 : IFC_FP32;
     c.criterion = IFC_SOLVER_CRITERION;
+    c.convection_scheme = IFC_SOLVER_CONVECTION;
     c.log_level = 1;
     return c;
 }

@@ -9,7 +9,9 @@ Configurations are dicts keyed by the reference's config.h names
 dynamicViscosity, velBC_type, velBC_val, numOuterIter, nIter_u/v/w/p,
 relax_u/v/w/p, tol_u/v/w/p, tol_mass`` plus the additions ``precision``
 ("f"/"d"), ``linear_solver``, ``criterion``, ``pin_pressure``,
-``sweeps_per_pass``, ``log_level`` and ``inlet_profile``.
+``sweeps_per_pass``, ``log_level``, ``inlet_profile`` and
+``convection_scheme`` (a CONV_* value or its name: "upwind", "central",
+"sou", "quick", "minmod", "van_leer").
 """
 from __future__ import annotations
 
@@ -26,6 +28,9 @@ EAST, WEST, NORTH, SOUTH, TOP, BOTTOM = range(6)
 WALL, INLET, OUTLET = range(3)
 GAUSS_SEIDEL, JACOBI = 0, 1
 CRIT_REFERENCE, CRIT_PER_FIELD = 0, 1
+CONV_UPWIND, CONV_CENTRAL, CONV_SOU, CONV_QUICK, CONV_MINMOD, CONV_VAN_LEER = range(6)
+CONV_NAMES = {"upwind": CONV_UPWIND, "central": CONV_CENTRAL, "sou": CONV_SOU, "quick": CONV_QUICK,
+              "minmod": CONV_MINMOD, "van_leer": CONV_VAN_LEER}
 FIELDS = ["u", "v", "w", "p", "T", "pc", "uf", "vf", "wf", "ac", "mcoef", "pcoef",
           "src_u", "src_v", "src_w", "src_p"]
 STAGES = ["face_bc", "mom_assemble", "mom_solve", "rhie_chow", "pcorr_coef", "pcorr_solve", "update"]
@@ -48,6 +53,7 @@ class IfcConfig(C.Structure):
         ("precision", C.c_int), ("linear_solver", C.c_int), ("criterion", C.c_int),
         ("pin_pressure", C.c_int), ("sweeps_per_pass", C.c_int), ("log_level", C.c_int),
         ("inlet_profile", C.POINTER(C.c_double)), ("stream", C.c_void_p),
+        ("convection_scheme", C.c_int),
     ]
 
 
@@ -247,6 +253,8 @@ def make_struct(cfg: dict) -> tuple[IfcConfig, object]:
     c.pin_pressure = int(cfg.get("pin_pressure", -1))
     c.sweeps_per_pass = int(cfg.get("sweeps_per_pass", 0))
     c.log_level = int(cfg.get("log_level", 0))
+    conv = cfg.get("convection_scheme", CONV_UPWIND)
+    c.convection_scheme = CONV_NAMES[conv] if isinstance(conv, str) else int(conv)
     if cfg.get("stream"):
         c.stream = C.c_void_p(int(cfg["stream"]))
     keep = None

@@ -46,6 +46,9 @@ enum { ORC_GS_LEX = 0, ORC_GS_REDBLACK = 1, ORC_JACOBI = 2 };
 enum { ORC_CRIT_REFERENCE = 0, ORC_CRIT_PER_FIELD = 1 };
 /* Equation ids for the linear solves. */
 enum { ORC_EQ_U = 0, ORC_EQ_V = 1, ORC_EQ_W = 2, ORC_EQ_P = 3 };
+/* Convection schemes; every scheme but upwind is applied by deferred correction. */
+enum { ORC_CONV_UPWIND = 0, ORC_CONV_CENTRAL = 1, ORC_CONV_SOU = 2, ORC_CONV_QUICK = 3, ORC_CONV_MINMOD = 4,
+       ORC_CONV_VAN_LEER = 5 };
 
 typedef struct orc_config {
     int dim, nx, ny, nz;
@@ -63,6 +66,7 @@ typedef struct orc_config {
     int criterion;          /* ORC_CRIT_REFERENCE / ORC_CRIT_PER_FIELD */
     int pin_pressure;       /* subtract the FP64 mean of p' (closed domains) */
     const double *inlet_profile; /* optional: west-face normal velocity per boundary cell (ny*nz) */
+    int convection;         /* ORC_CONV_*; 0 = first-order upwind, the reference's only scheme */
 } orc_config;
 
 /* Per-outer-iteration norms (RMS, FP64), src/Solver.cu:226-235. */
@@ -92,6 +96,7 @@ enum {
     void orc_mom_link_coef_##S(orc_state_##S *s);                                          \
     void orc_mom_src_##S(orc_state_##S *s);                                                \
     void orc_bc_mom_##S(orc_state_##S *s);                                                 \
+    void orc_dc_source_##S(orc_state_##S *s);                                              \
     double orc_sweep_##S(orc_state_##S *s, int eq, int mode);                              \
     int orc_linear_solve_##S(orc_state_##S *s, int eq, double *sweep_norms);               \
     void orc_rhie_chow_##S(orc_state_##S *s);                                              \

@@ -266,6 +266,108 @@ void FN(bc_mom)(ST *s)
 #undef BCV
 }
 
+/* Higher-order convection by deferred correction (Khosla & Rubin 1974).  Not in
+ * the reference, whose convection is first-order upwind only
+ * (include/kernels.cuh:97-134; README.md:412 lists higher-order schemes as
+ * planned).  The links stay upwind; the difference between a higher-order face
+ * value and the upwind one, times the face's mass flux, enters the source,
+ * evaluated with the fields at the start of the outer iteration:
+ *   b_C += sum over faces f of -F_f,out (phi_f - phi_U,f).
+ * With phi_U the upwind cell, phi_D the downwind cell and phi_UU the cell
+ * beyond phi_U, dd = phi_D - phi_U and du = phi_U - phi_UU, the face value is
+ * phi_f = phi_U + 0.5 L(du, dd):
+ *   central                 L = dd
+ *   second-order upwind     L = du
+ *   QUICK (Leonard 1979)    L = (3 dd + du) / 4
+ *   minmod (Roe 1986)       L = du or dd, the smaller in magnitude, if du dd > 0, else 0
+ *   van Leer (1974)         L = 2 du dd / (du + dd) if du dd > 0, else 0
+ * Boundary faces, and faces whose far-upwind cell lies outside the domain,
+ * keep the upwind value.  Face quantity Q = (rho u_f A) * (0.5 L); a cell's
+ * correction is (Q_w - Q_e) + (Q_s - Q_n) [+ (Q_b - Q_t)], added to its source
+ * after the boundary fold-in. */
+static inline T CAT(dc_limit_, S)(int scheme, T du, T dd)
+{
+    switch (scheme) {
+    case ORC_CONV_CENTRAL: return dd;
+    case ORC_CONV_SOU: return du;
+    case ORC_CONV_QUICK: return ((T)3 * dd + du) / (T)4;
+    case ORC_CONV_MINMOD:
+        if (!(du * dd > (T)0)) return (T)0;
+        return fabs((double)du) < fabs((double)dd) ? du : dd;
+    case ORC_CONV_VAN_LEER:
+        if (!(du * dd > (T)0)) return (T)0;
+        return (T)2 * du * dd / (du + dd);
+    default: return (T)0;
+    }
+}
+
+/* Q of one interior face between cells L and R along one axis; ll / rr are the
+ * cells beyond L and R (has_ll / has_rr: inside the domain). */
+static inline T CAT(dc_face_, S)(int scheme, T rho, T uf, T A, T pll, T pl, T pr, T prr, int has_ll, int has_rr)
+{
+    const T F = rho * uf * A;
+    T U, D, UU;
+    if (F > (T)0) {
+        if (!has_ll) return (T)0;
+        U = pl; D = pr; UU = pll;
+    } else if (F < (T)0) {
+        if (!has_rr) return (T)0;
+        U = pr; D = pl; UU = prr;
+    } else {
+        return (T)0;
+    }
+    return F * ((T)0.5 * CAT(dc_limit_, S)(scheme, U - UU, D - U));
+}
+
+static T CAT(dc_cell_, S)(const ST *s, const T *phi, int i, int j, int k)
+{
+    const int sc = s->cfg.convection, nx = s->nx, ny = s->ny, nz = s->nz;
+    const T *uf = s->f[ORC_F_UF], *vf = s->f[ORC_F_VF], *wf = s->f[ORC_F_WF];
+    const T rho = s->rho;
+#define PH(a, b, c) phi[CID(s, a, b, c)]
+    T qw = (T)0, qe = (T)0, qs = (T)0, qn = (T)0, qb = (T)0, qt = (T)0;
+    if (i > 0)
+        qw = CAT(dc_face_, S)(sc, rho, uf[UFID(s, i, j, k)], s->Ax, i > 1 ? PH(i - 2, j, k) : (T)0, PH(i - 1, j, k),
+                              PH(i, j, k), i < nx - 1 ? PH(i + 1, j, k) : (T)0, i > 1, i < nx - 1);
+    if (i < nx - 1)
+        qe = CAT(dc_face_, S)(sc, rho, uf[UFID(s, i + 1, j, k)], s->Ax, i > 0 ? PH(i - 1, j, k) : (T)0, PH(i, j, k),
+                              PH(i + 1, j, k), i < nx - 2 ? PH(i + 2, j, k) : (T)0, i > 0, i < nx - 2);
+    if (j > 0)
+        qs = CAT(dc_face_, S)(sc, rho, vf[VFID(s, i, j, k)], s->Ay, j > 1 ? PH(i, j - 2, k) : (T)0, PH(i, j - 1, k),
+                              PH(i, j, k), j < ny - 1 ? PH(i, j + 1, k) : (T)0, j > 1, j < ny - 1);
+    if (j < ny - 1)
+        qn = CAT(dc_face_, S)(sc, rho, vf[VFID(s, i, j + 1, k)], s->Ay, j > 0 ? PH(i, j - 1, k) : (T)0, PH(i, j, k),
+                              PH(i, j + 1, k), j < ny - 2 ? PH(i, j + 2, k) : (T)0, j > 0, j < ny - 2);
+    T dc = (qw - qe) + (qs - qn);
+    if (s->dim == 3) {
+        if (k > 0)
+            qb = CAT(dc_face_, S)(sc, rho, wf[WFID(s, i, j, k)], s->Az, k > 1 ? PH(i, j, k - 2) : (T)0,
+                                  PH(i, j, k - 1), PH(i, j, k), k < nz - 1 ? PH(i, j, k + 1) : (T)0, k > 1, k < nz - 1);
+        if (k < nz - 1)
+            qt = CAT(dc_face_, S)(sc, rho, wf[WFID(s, i, j, k + 1)], s->Az, k > 0 ? PH(i, j, k - 1) : (T)0,
+                                  PH(i, j, k), PH(i, j, k + 1), k < nz - 2 ? PH(i, j, k + 2) : (T)0, k > 0, k < nz - 2);
+        dc = dc + (qb - qt);
+    }
+#undef PH
+    return dc;
+}
+
+/* Adds the deferred-correction source of every momentum component (u, v, w
+ * all at the start-of-iteration fields) to src_u, src_v, src_w. */
+void FN(dc_source)(ST *s)
+{
+    if (s->cfg.convection == ORC_CONV_UPWIND) return;
+    const int nc = s->dim;
+    const int fphi[3] = {ORC_F_U, ORC_F_V, ORC_F_W}, fsrc[3] = {ORC_F_SRC_U, ORC_F_SRC_V, ORC_F_SRC_W};
+    for (int c = 0; c < nc; ++c) {
+        T *b = s->f[fsrc[c]];
+        for (int k = 0; k < s->nz; ++k)
+            for (int j = 0; j < s->ny; ++j)
+                for (int i = 0; i < s->nx; ++i) s->tmp[CID(s, i, j, k)] = CAT(dc_cell_, S)(s, s->f[fphi[c]], i, j, k);
+        for (size_t id = 0; id < s->N; ++id) b[id] = b[id] + s->tmp[id];
+    }
+}
+
 /* One relaxed point update, include/kernels.cuh:935-988 (GaussSeidelIterateKernel)
  * and :854-907 (pointJacobiIterateKernel): out-of-domain neighbours are 0,
  * phi_new = (b - sum a_nb phi_nb) / aC, phi += relax (phi_new - phi). */
@@ -560,6 +662,7 @@ int FN(outer_iteration)(ST *s, orc_norms *out)
     FN(mom_link_coef)(s);
     FN(mom_src)(s);
     FN(bc_mom)(s);
+    FN(dc_source)(s);
     nm.sweeps[ORC_EQ_U] = FN(linear_solve)(s, ORC_EQ_U, NULL);
     nm.sweeps[ORC_EQ_V] = FN(linear_solve)(s, ORC_EQ_V, NULL);
     if (s->dim == 3) nm.sweeps[ORC_EQ_W] = FN(linear_solve)(s, ORC_EQ_W, NULL);

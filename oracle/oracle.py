@@ -23,6 +23,9 @@ LIB_PATH = os.path.join(HERE, "_build", "libifc_oracle.so")
 GS_LEX, GS_REDBLACK, JACOBI = 0, 1, 2
 CRIT_REFERENCE, CRIT_PER_FIELD = 0, 1
 EQ_U, EQ_V, EQ_W, EQ_P = 0, 1, 2, 3
+# Convection schemes (0 is the reference's first-order upwind; the others are
+# applied by deferred correction).
+CONV = {"upwind": 0, "central": 1, "sou": 2, "quick": 3, "minmod": 4, "van_leer": 5}
 FIELDS = ["u", "v", "w", "p", "pc", "uf", "vf", "wf", "mcoef", "pcoef", "src_u", "src_v", "src_w", "src_p"]
 
 
@@ -37,6 +40,7 @@ class OrcConfig(C.Structure):
         ("relax", C.c_double * 4), ("tol", C.c_double * 4), ("tol_mass", C.c_double),
         ("sweep_mode", C.c_int), ("check_every", C.c_int), ("criterion", C.c_int),
         ("pin_pressure", C.c_int), ("inlet_profile", C.POINTER(C.c_double)),
+        ("convection", C.c_int),
     ]
 
 
@@ -77,7 +81,7 @@ def lib():
                 "create": (P, [C.POINTER(OrcConfig)]), "destroy": (None, [P]),
                 "field": (C.POINTER(T), [P, C.c_int]), "field_len": (C.c_size_t, [P, C.c_int]),
                 "init_face_vel": (None, [P]), "bc_face_vel": (None, [P]), "mom_link_coef": (None, [P]),
-                "mom_src": (None, [P]), "bc_mom": (None, [P]), "sweep": (C.c_double, [P, C.c_int, C.c_int]),
+                "mom_src": (None, [P]), "bc_mom": (None, [P]), "dc_source": (None, [P]), "sweep": (C.c_double, [P, C.c_int, C.c_int]),
                 "linear_solve": (C.c_int, [P, C.c_int, C.POINTER(C.c_double)]),
                 "rhie_chow": (None, [P]), "pcorr_link_coef": (None, [P]), "pcorr_src": (C.c_double, [P]),
                 "pin_pcorr": (None, [P]), "update_field": (None, [P, C.POINTER(OrcNorms)]),
@@ -121,6 +125,8 @@ def make_struct(cfg: dict) -> tuple[OrcConfig, object]:
     c.check_every = int(cfg.get("check_every", 1))
     c.criterion = int(cfg.get("criterion", CRIT_PER_FIELD))
     c.pin_pressure = int(cfg.get("pin_pressure", 0))
+    conv = cfg.get("convection_scheme", 0)
+    c.convection = CONV[conv] if isinstance(conv, str) else int(conv)
     keep = None
     prof = cfg.get("inlet_profile")
     if prof is not None:
@@ -172,6 +178,7 @@ class Oracle:
     def mom_link_coef(self): self._fn("mom_link_coef")(self._h)
     def mom_src(self): self._fn("mom_src")(self._h)
     def bc_mom(self): self._fn("bc_mom")(self._h)
+    def dc_source(self): self._fn("dc_source")(self._h)
     def rhie_chow(self): self._fn("rhie_chow")(self._h)
     def pcorr_link_coef(self): self._fn("pcorr_link_coef")(self._h)
     def pcorr_src(self) -> float: return self._fn("pcorr_src")(self._h)
@@ -214,6 +221,7 @@ class AdjointOracle(Oracle):
     (orc_adjoint_apply_d) and the adjoint fixed-point solve built on it."""
 
     def __init__(self, cfg: dict):
+        assert cfg.get("convection_scheme", 0) in (0, "upwind"), "the adjoint linearises upwind convection only"
         super().__init__(cfg, "d")
 
     def state_sizes(self):
