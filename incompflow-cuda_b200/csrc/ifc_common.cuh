@@ -84,6 +84,31 @@ struct Ctl {
     LogRec log[kLogCap];
 };
 
+// ---- row-segment work units ------------------------------------------------
+// The cell-wise kernels below hand one warp a segment of kRowSeg consecutive
+// cells of one x-row (row r = j + ny*k), lanes strided along x: the row and
+// segment come from one division per unit instead of per cell, a warp's loads
+// are contiguous, and small-ny grids still yield many units.
+constexpr int kRowSeg = 128;
+
+__host__ __device__ __forceinline__ int row_units(int nx, int rows) { return rows * ((nx + kRowSeg - 1) / kRowSeg); }
+
+struct RowUnit {
+    int r, j, k, i0, i1;  // row, its j and k, cells [i0, i1)
+};
+
+__device__ __forceinline__ RowUnit row_unit(int u, int nx, int ny)
+{
+    const int nseg = (nx + kRowSeg - 1) / kRowSeg;
+    RowUnit w;
+    w.r = u / nseg;
+    w.i0 = (u - w.r * nseg) * kRowSeg;
+    w.i1 = min(w.i0 + kRowSeg, nx);
+    w.j = w.r % ny;
+    w.k = w.r / ny;
+    return w;
+}
+
 // ---- deterministic FP64 reduction over the whole grid --------------------
 // Every block reduces its values, writes one partial per value, and the last
 // block to arrive sums all partials in a fixed order.  The result therefore

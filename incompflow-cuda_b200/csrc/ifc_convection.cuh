@@ -71,57 +71,83 @@ __host__ __device__ __forceinline__ T dc_face(int scheme, T rho, T uf, T A, T pl
     return F * ((T)0.5 * dc_limit<T>(scheme, U - UU, D - U));
 }
 
-// Correction of cell (i, j, k) for the field phi (global, cell layout), with
-// the face velocities of f.
+// Correction of cell c = (i, j, k) for the field phi (global, cell layout),
+// given the velocities of the cell's six faces (west, east, south, north,
+// bottom, top).
 template <typename T, int DIM>
-__device__ __forceinline__ T dc_cell(const Params<T> &P, const Fields<T> &f, const T *phi, int i, int j, int k)
+__device__ __forceinline__ T dc_cell(const Geo<T> &g, const T *phi, int c, int i, int j, int k, T uw, T ue, T vs,
+                                     T vn, T wb, T wt)
 {
-    const Geo<T> &g = P.g;
     const int sc = g.conv, nx = g.nx, ny = g.ny, nz = g.nz;
-    const int c = i + nx * (j + ny * k);
     const int sx = 1, sy = nx, sz = nx * ny;
     const T rho = g.rho;
     T qw = (T)0, qe = (T)0, qs = (T)0, qn = (T)0;
-    const int fu = i + (nx + 1) * (j + ny * k);
-    const int fv = i + nx * (j + (ny + 1) * k);
     if (i > 0)
-        qw = dc_face<T>(sc, rho, f.uf[fu], g.Ax, i > 1 ? phi[c - 2 * sx] : (T)0, phi[c - sx], phi[c],
+        qw = dc_face<T>(sc, rho, uw, g.Ax, i > 1 ? phi[c - 2 * sx] : (T)0, phi[c - sx], phi[c],
                         i < nx - 1 ? phi[c + sx] : (T)0, i > 1, i < nx - 1);
     if (i < nx - 1)
-        qe = dc_face<T>(sc, rho, f.uf[fu + 1], g.Ax, i > 0 ? phi[c - sx] : (T)0, phi[c], phi[c + sx],
+        qe = dc_face<T>(sc, rho, ue, g.Ax, i > 0 ? phi[c - sx] : (T)0, phi[c], phi[c + sx],
                         i < nx - 2 ? phi[c + 2 * sx] : (T)0, i > 0, i < nx - 2);
     if (j > 0)
-        qs = dc_face<T>(sc, rho, f.vf[fv], g.Ay, j > 1 ? phi[c - 2 * sy] : (T)0, phi[c - sy], phi[c],
+        qs = dc_face<T>(sc, rho, vs, g.Ay, j > 1 ? phi[c - 2 * sy] : (T)0, phi[c - sy], phi[c],
                         j < ny - 1 ? phi[c + sy] : (T)0, j > 1, j < ny - 1);
     if (j < ny - 1)
-        qn = dc_face<T>(sc, rho, f.vf[fv + nx], g.Ay, j > 0 ? phi[c - sy] : (T)0, phi[c], phi[c + sy],
+        qn = dc_face<T>(sc, rho, vn, g.Ay, j > 0 ? phi[c - sy] : (T)0, phi[c], phi[c + sy],
                         j < ny - 2 ? phi[c + 2 * sy] : (T)0, j > 0, j < ny - 2);
     T dc = (qw - qe) + (qs - qn);
     if (DIM == 3) {
         T qb = (T)0, qt = (T)0;
         if (k > 0)
-            qb = dc_face<T>(sc, rho, f.wf[c], g.Az, k > 1 ? phi[c - 2 * sz] : (T)0, phi[c - sz], phi[c],
+            qb = dc_face<T>(sc, rho, wb, g.Az, k > 1 ? phi[c - 2 * sz] : (T)0, phi[c - sz], phi[c],
                             k < nz - 1 ? phi[c + sz] : (T)0, k > 1, k < nz - 1);
         if (k < nz - 1)
-            qt = dc_face<T>(sc, rho, f.wf[c + sz], g.Az, k > 0 ? phi[c - sz] : (T)0, phi[c], phi[c + sz],
+            qt = dc_face<T>(sc, rho, wt, g.Az, k > 0 ? phi[c - sz] : (T)0, phi[c], phi[c + sz],
                             k < nz - 2 ? phi[c + 2 * sz] : (T)0, k > 0, k < nz - 2);
         dc = dc + (qb - qt);
     }
     return dc;
 }
 
+// The same with the face velocities read from f.
+template <typename T, int DIM>
+__device__ __forceinline__ T dc_cell(const Params<T> &P, const Fields<T> &f, const T *phi, int i, int j, int k)
+{
+    const Geo<T> &g = P.g;
+    const int nx = g.nx, ny = g.ny;
+    const int c = i + nx * (j + ny * k);
+    const int fu = i + (nx + 1) * (j + ny * k), fv = i + nx * (j + (ny + 1) * k);
+    const T wb = DIM == 3 ? f.wf[c] : (T)0, wt = DIM == 3 ? f.wf[c + nx * ny] : (T)0;
+    return dc_cell<T, DIM>(g, phi, c, i, j, k, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], wb, wt);
+}
+
 // f.sdc[q*N + id] = correction of momentum component q (u, v, w) at cell id,
-// from the current u, v, w and face velocities.  One thread per cell.
+// from the current u, v, w and face velocities; row-segment work units (the
+// six face velocities are read once for the three components).
 template <typename T, int DIM>
 __global__ void k_dc_source(Params<T> P, Fields<T> f)
 {
-    const int N = P.g.N, nx = P.g.nx, ny = P.g.ny;
-    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
-        const int i = id % nx, j = (id / nx) % ny, k = id / (nx * ny);
-        f.sdc[id] = dc_cell<T, DIM>(P, f, f.u, i, j, k);
-        f.sdc[(size_t)N + id] = dc_cell<T, DIM>(P, f, f.v, i, j, k);
-        if (DIM == 3) f.sdc[2 * (size_t)N + id] = dc_cell<T, DIM>(P, f, f.w, i, j, k);
+    const Geo<T> &g = P.g;
+    const int N = g.N, nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int units = row_units(nx, ny * nz);
+    for (int u = gw; u < units; u += nw) {
+        const RowUnit w = row_unit(u, nx, ny);
+        const int c0 = nx * w.r, f0 = (nx + 1) * w.r, v0 = nx * (w.j + (ny + 1) * w.k);
+        for (int i = w.i0 + lane; i < w.i1; i += 32) {
+            const int c = c0 + i;
+            const T uw = f.uf[f0 + i], ue = f.uf[f0 + i + 1], vs = f.vf[v0 + i], vn = f.vf[v0 + i + nx];
+            const T wb = DIM == 3 ? f.wf[c] : (T)0, wt = DIM == 3 ? f.wf[c + pl] : (T)0;
+            const T du = dc_cell<T, DIM>(g, f.u, c, i, w.j, w.k, uw, ue, vs, vn, wb, wt);
+            const T dv = dc_cell<T, DIM>(g, f.v, c, i, w.j, w.k, uw, ue, vs, vn, wb, wt);
+            T dw = (T)0;
+            if (DIM == 3) dw = dc_cell<T, DIM>(g, f.w, c, i, w.j, w.k, uw, ue, vs, vn, wb, wt);
+            f.sdc[c] = du;
+            f.sdc[(size_t)N + c] = dv;
+            if (DIM == 3) f.sdc[2 * (size_t)N + c] = dw;
+        }
     }
+    (void)nz;
 }
 
 }  // namespace ifc

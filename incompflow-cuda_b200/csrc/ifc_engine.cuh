@@ -147,6 +147,9 @@ struct Engine : EngineBase {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
+    // Blocks of 256 threads for the row-segment kernels (one warp per unit).
+    int row_grid() const { return grid(32LL * row_units(P.g.nx, P.g.ny * P.g.nz)); }
+
     int grid(long long work) const
     {
         long long b = (work + 255) / 256;
@@ -444,7 +447,7 @@ struct Engine : EngineBase {
     void enq_dc_source()
     {
         if (P.g.conv == CONV_UPWIND) return;
-        k_dc_source<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f);
+        k_dc_source<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f);
         ++launches;
     }
 
@@ -493,9 +496,8 @@ struct Engine : EngineBase {
             enq_fused_rc();
             return;
         }
-        const long long nf = (long long)nface(0) + nface(1) + (DIM == 3 ? (long long)nface(2) : 0);
-        k_rhie_chow<T, DIM><<<grid(nf), 256, 0, stream>>>(P, f);
-        k_pcorr_src<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl, partials);
+        k_rhie_chow<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f);
+        k_pcorr_src<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f, ctl, partials);
         launches += 2;
     }
 
@@ -547,7 +549,7 @@ struct Engine : EngineBase {
     template <int DIM>
     void enq_update(int use_cond)
     {
-        k_update<T, DIM><<<grid(P.g.N), 256, 0, stream>>>(P, f, ctl, partials, cond, use_cond);
+        k_update<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f, ctl, partials, cond, use_cond);
         ++launches;
     }
 

@@ -244,54 +244,56 @@ __global__ void k_rhie_chow(Params<T> P, Fields<T> f)
 {
     const Geo<T> &g = P.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
-    const long long nuf = (long long)(nx + 1) * ny * nz, nvf = (long long)nx * (ny + 1) * nz;
-    const long long nwf = DIM == 3 ? (long long)pl * (nz + 1) : 0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nuf + nvf + nwf;
-         q += (long long)gridDim.x * blockDim.x) {
-        if (q < nuf) {
-            int i = (int)(q % (nx + 1));
-            int r = (int)(q / (nx + 1));
-            int R = i + nx * r, L = R - 1;
-            T val;
-            if (i == 0) val = face_bc(g, WEST, 0, f.u[R], r);
-            else if (i == nx) val = face_bc(g, EAST, 0, f.u[L], r);
-            else {
-                T pL = f.p[L], pR = f.p[R];
-                T pLL = i >= 2 ? f.p[L - 1] : (g.closed[WEST] ? pL : (T)0);
-                T pRR = i <= nx - 2 ? f.p[R + 1] : (g.closed[EAST] ? pR : (T)0);
-                val = rc_face(f.u[L], f.u[R], f.ac[L], f.ac[R], pLL, pL, pR, pRR, g.Ax);
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int units = row_units(nx, ny * nz);
+    for (int u = gw; u < units; u += nw) {
+        const RowUnit w = row_unit(u, nx, ny);
+        const int j = w.j, k = w.k, r = w.r, c0 = nx * r, f0 = (nx + 1) * r, v0 = nx * (j + (ny + 1) * k);
+        for (int i = w.i0 + lane; i < w.i1; i += 32) {
+            const int R = c0 + i;
+            // x-face i of the row (west face of cell i)
+            {
+                const int L = R - 1;
+                T val;
+                if (i == 0) val = face_bc(g, WEST, 0, f.u[R], r);
+                else {
+                    T pL = f.p[L], pR = f.p[R];
+                    T pLL = i >= 2 ? f.p[L - 1] : (g.closed[WEST] ? pL : (T)0);
+                    T pRR = i <= nx - 2 ? f.p[R + 1] : (g.closed[EAST] ? pR : (T)0);
+                    val = rc_face(f.u[L], f.u[R], f.ac[L], f.ac[R], pLL, pL, pR, pRR, g.Ax);
+                }
+                f.uf[f0 + i] = val;
+                if (i == nx - 1) f.uf[f0 + nx] = face_bc(g, EAST, 0, f.u[R], r);
             }
-            f.uf[q] = val;
-        } else if (q < nuf + nvf) {
-            long long qq = q - nuf;
-            int i = (int)(qq % nx);
-            int j = (int)((qq / nx) % (ny + 1));
-            int k = (int)(qq / ((long long)nx * (ny + 1)));
-            int R = i + nx * (j + ny * k), L = R - nx;
-            T val;
-            if (j == 0) val = face_bc(g, SOUTH, 1, f.v[R], 0);
-            else if (j == ny) val = face_bc(g, NORTH, 1, f.v[L], 0);
-            else {
-                T pL = f.p[L], pR = f.p[R];
-                T pLL = j >= 2 ? f.p[L - nx] : (g.closed[SOUTH] ? pL : (T)0);
-                T pRR = j <= ny - 2 ? f.p[R + nx] : (g.closed[NORTH] ? pR : (T)0);
-                val = rc_face(f.v[L], f.v[R], f.ac[L], f.ac[R], pLL, pL, pR, pRR, g.Ay);
+            // y-face j of the column (south face of cell (i, j))
+            {
+                const int L = R - nx;
+                T val;
+                if (j == 0) val = face_bc(g, SOUTH, 1, f.v[R], 0);
+                else {
+                    T pL = f.p[L], pR = f.p[R];
+                    T pLL = j >= 2 ? f.p[L - nx] : (g.closed[SOUTH] ? pL : (T)0);
+                    T pRR = j <= ny - 2 ? f.p[R + nx] : (g.closed[NORTH] ? pR : (T)0);
+                    val = rc_face(f.v[L], f.v[R], f.ac[L], f.ac[R], pLL, pL, pR, pRR, g.Ay);
+                }
+                f.vf[v0 + i] = val;
+                if (j == ny - 1) f.vf[v0 + nx + i] = face_bc(g, NORTH, 1, f.v[R], 0);
             }
-            f.vf[qq] = val;
-        } else {
-            long long qq = q - nuf - nvf;
-            int k = (int)(qq / pl);
-            int R = (int)qq, L = R - pl;
-            T val;
-            if (k == 0) val = face_bc(g, BOTTOM, 2, f.w[R], 0);
-            else if (k == nz) val = face_bc(g, TOP, 2, f.w[L], 0);
-            else {
-                T pL = f.p[L], pR = f.p[R];
-                T pLL = k >= 2 ? f.p[L - pl] : (g.closed[BOTTOM] ? pL : (T)0);
-                T pRR = k <= nz - 2 ? f.p[R + pl] : (g.closed[TOP] ? pR : (T)0);
-                val = rc_face(f.w[L], f.w[R], f.ac[L], f.ac[R], pLL, pL, pR, pRR, g.Az);
+            // z-face k (bottom face of cell (i, j, k))
+            if (DIM == 3) {
+                const int L = R - pl;
+                T val;
+                if (k == 0) val = face_bc(g, BOTTOM, 2, f.w[R], 0);
+                else {
+                    T pL = f.p[L], pR = f.p[R];
+                    T pLL = k >= 2 ? f.p[L - pl] : (g.closed[BOTTOM] ? pL : (T)0);
+                    T pRR = k <= nz - 2 ? f.p[R + pl] : (g.closed[TOP] ? pR : (T)0);
+                    val = rc_face(f.w[L], f.w[R], f.ac[L], f.ac[R], pLL, pL, pR, pRR, g.Az);
+                }
+                f.wf[R] = val;
+                if (k == nz - 1) f.wf[R + pl] = face_bc(g, TOP, 2, f.w[R], 0);
             }
-            f.wf[qq] = val;
         }
     }
 }
@@ -301,15 +303,21 @@ template <typename T, int DIM>
 __global__ void k_pcorr_src(Params<T> P, Fields<T> f, Ctl *ctl, double *partials)
 {
     const Geo<T> &g = P.g;
-    const int N = g.N, nx = g.nx, ny = g.ny, pl = nx * ny;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int units = row_units(nx, ny * nz);
     double s[1] = {0.0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) {
-        int i = c % nx, j = (c / nx) % ny, k = c / pl;
-        int fu = i + (nx + 1) * (j + ny * k), fv = i + nx * (j + (ny + 1) * k);
-        T wb = DIM == 3 ? f.wf[c] : (T)0, wt = DIM == 3 ? f.wf[c + pl] : (T)0;
-        T b = mass_imbalance<T, DIM>(g, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], wb, wt);
-        f.sp[c] = b;
-        s[0] += (double)b * (double)b;
+    for (int u = gw; u < units; u += nw) {
+        const RowUnit w = row_unit(u, nx, ny);
+        const int c0 = nx * w.r, f0 = (nx + 1) * w.r, v0 = nx * (w.j + (ny + 1) * w.k);
+        for (int i = w.i0 + lane; i < w.i1; i += 32) {
+            const int c = c0 + i;
+            T wb = DIM == 3 ? f.wf[c] : (T)0, wt = DIM == 3 ? f.wf[c + pl] : (T)0;
+            T b = mass_imbalance<T, DIM>(g, f.uf[f0 + i], f.uf[f0 + i + 1], f.vf[v0 + i], f.vf[v0 + i + nx], wb, wt);
+            f.sp[c] = b;
+            s[0] += (double)b * (double)b;
+        }
     }
     __shared__ double tot[1];
     if (grid_reduce<1>(s, partials, ctl, tot) && threadIdx.x == 0) ctl->sq[SQ_MASS] = tot[0];
@@ -456,61 +464,84 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
 }
 
 // ---- corrections, kernels.cuh:583-843 ---------------------------------------
+// 64 registers (4 blocks of 256 per SM): the loads-first body otherwise takes
+// ~100 and halves the warps in flight of this memory-bound kernel.
 template <typename T, int DIM>
-__global__ void k_update(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, cudaGraphConditionalHandle cond,
+__global__ void __launch_bounds__(256, 4) k_update(Params<T> P, Fields<T> f, Ctl *ctl, double *partials, cudaGraphConditionalHandle cond,
                          int use_cond)
 {
     const Geo<T> &g = P.g;
-    const int N = g.N, nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int units = row_units(nx, ny * nz);
     double s[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) {
-        int i = c % nx, j = (c / nx) % ny, k = c / pl;
-        const T pc = f.pc[c], aC = f.ac[c];
-        T dp = g.relax[EQ_P] * pc;
-        f.p[c] += dp;
-        s[0] += (double)dp * (double)dp;
-        T L = i > 0 ? f.pc[c - 1] : (g.closed[WEST] ? pc : (T)0);
-        T R = i < nx - 1 ? f.pc[c + 1] : (g.closed[EAST] ? pc : (T)0);
-        T d = vel_corr(P.d.ru[0], L, R, g.Ax, aC);
-        const T un = f.u[c] + d;
-        f.u[c] = un;
-        s[1] += (double)d * (double)d;
-        // Boundary faces of the next outer iteration (kernels.cuh:47-95 with
-        // the corrected velocities, src/Solver.cu:165).
-        if (i == 0) f.uf[(nx + 1) * (j + ny * k)] = face_bc(g, WEST, 0, un, j + ny * k);
-        if (i == nx - 1) f.uf[nx + (nx + 1) * (j + ny * k)] = face_bc(g, EAST, 0, un, j + ny * k);
-        L = j > 0 ? f.pc[c - nx] : (g.closed[SOUTH] ? pc : (T)0);
-        R = j < ny - 1 ? f.pc[c + nx] : (g.closed[NORTH] ? pc : (T)0);
-        d = vel_corr(P.d.ru[1], L, R, g.Ay, aC);
-        const T vn = f.v[c] + d;
-        f.v[c] = vn;
-        s[2] += (double)d * (double)d;
-        if (j == 0) f.vf[i + nx * ((ny + 1) * k)] = face_bc(g, SOUTH, 1, vn, 0);
-        if (j == ny - 1) f.vf[i + nx * (ny + (ny + 1) * k)] = face_bc(g, NORTH, 1, vn, 0);
-        if (DIM == 3) {
-            L = k > 0 ? f.pc[c - pl] : (g.closed[BOTTOM] ? pc : (T)0);
-            R = k < nz - 1 ? f.pc[c + pl] : (g.closed[TOP] ? pc : (T)0);
-            d = vel_corr(P.d.ru[2], L, R, g.Az, aC);
-            const T wn = f.w[c] + d;
-            f.w[c] = wn;
-            s[3] += (double)d * (double)d;
-            if (k == 0) f.wf[c] = face_bc(g, BOTTOM, 2, wn, 0);
-            if (k == nz - 1) f.wf[c + pl] = face_bc(g, TOP, 2, wn, 0);
-        }
-        if (i >= 1) {
-            d = face_corr(P.d.ru[0], f.ac[c - 1], aC, f.pc[c - 1], pc, g.Ax);
-            f.uf[i + (nx + 1) * (j + ny * k)] += d;
-            s[4] += (double)d * (double)d;
-        }
-        if (j >= 1) {
-            d = face_corr(P.d.ru[1], f.ac[c - nx], aC, f.pc[c - nx], pc, g.Ay);
-            f.vf[i + nx * (j + (ny + 1) * k)] += d;
-            s[5] += (double)d * (double)d;
-        }
-        if (DIM == 3 && k >= 1) {
-            d = face_corr(P.d.ru[2], f.ac[c - pl], aC, f.pc[c - pl], pc, g.Az);
-            f.wf[c] += d;
-            s[6] += (double)d * (double)d;
+    for (int u = gw; u < units; u += nw) {
+        const RowUnit w = row_unit(u, nx, ny);
+        const int j = w.j, k = w.k, r = w.r, c0 = nx * r, f0 = (nx + 1) * r, v0 = nx * (j + (ny + 1) * k);
+        for (int i = w.i0 + lane; i < w.i1; i += 32) {
+            const int c = c0 + i;
+            // every load of the cell first: no store below can alias them
+            const T pc = f.pc[c], aC = f.ac[c];
+            const T pcW = i > 0 ? f.pc[c - 1] : (T)0, pcE = i < nx - 1 ? f.pc[c + 1] : (T)0;
+            const T pcS = j > 0 ? f.pc[c - nx] : (T)0, pcN = j < ny - 1 ? f.pc[c + nx] : (T)0;
+            const T acW = i > 0 ? f.ac[c - 1] : (T)1, acS = j > 0 ? f.ac[c - nx] : (T)1;
+            const T p0 = f.p[c], u0 = f.u[c], v0c = f.v[c];
+            const T uf0 = i > 0 ? f.uf[f0 + i] : (T)0, vf0 = j > 0 ? f.vf[v0 + i] : (T)0;
+            T pcB = (T)0, pcT = (T)0, acB = (T)1, w0 = (T)0, wf0 = (T)0;
+            if (DIM == 3) {
+                pcB = k > 0 ? f.pc[c - pl] : (T)0;
+                pcT = k < nz - 1 ? f.pc[c + pl] : (T)0;
+                acB = k > 0 ? f.ac[c - pl] : (T)1;
+                w0 = f.w[c];
+                wf0 = k > 0 ? f.wf[c] : (T)0;
+            }
+            const T dp = g.relax[EQ_P] * pc;
+            f.p[c] = p0 + dp;
+            s[0] += (double)dp * (double)dp;
+            T L = i > 0 ? pcW : (g.closed[WEST] ? pc : (T)0);
+            T R = i < nx - 1 ? pcE : (g.closed[EAST] ? pc : (T)0);
+            T d = vel_corr(P.d.ru[0], L, R, g.Ax, aC);
+            const T un = u0 + d;
+            f.u[c] = un;
+            s[1] += (double)d * (double)d;
+            // Boundary faces of the next outer iteration (kernels.cuh:47-95 with
+            // the corrected velocities, src/Solver.cu:165).
+            if (i == 0) f.uf[f0] = face_bc(g, WEST, 0, un, r);
+            if (i == nx - 1) f.uf[f0 + nx] = face_bc(g, EAST, 0, un, r);
+            L = j > 0 ? pcS : (g.closed[SOUTH] ? pc : (T)0);
+            R = j < ny - 1 ? pcN : (g.closed[NORTH] ? pc : (T)0);
+            d = vel_corr(P.d.ru[1], L, R, g.Ay, aC);
+            const T vn = v0c + d;
+            f.v[c] = vn;
+            s[2] += (double)d * (double)d;
+            if (j == 0) f.vf[v0 + i] = face_bc(g, SOUTH, 1, vn, 0);
+            if (j == ny - 1) f.vf[v0 + nx + i] = face_bc(g, NORTH, 1, vn, 0);
+            if (DIM == 3) {
+                L = k > 0 ? pcB : (g.closed[BOTTOM] ? pc : (T)0);
+                R = k < nz - 1 ? pcT : (g.closed[TOP] ? pc : (T)0);
+                d = vel_corr(P.d.ru[2], L, R, g.Az, aC);
+                const T wn = w0 + d;
+                f.w[c] = wn;
+                s[3] += (double)d * (double)d;
+                if (k == 0) f.wf[c] = face_bc(g, BOTTOM, 2, wn, 0);
+                if (k == nz - 1) f.wf[c + pl] = face_bc(g, TOP, 2, wn, 0);
+            }
+            if (i >= 1) {
+                d = face_corr(P.d.ru[0], acW, aC, pcW, pc, g.Ax);
+                f.uf[f0 + i] = uf0 + d;
+                s[4] += (double)d * (double)d;
+            }
+            if (j >= 1) {
+                d = face_corr(P.d.ru[1], acS, aC, pcS, pc, g.Ay);
+                f.vf[v0 + i] = vf0 + d;
+                s[5] += (double)d * (double)d;
+            }
+            if (DIM == 3 && k >= 1) {
+                d = face_corr(P.d.ru[2], acB, aC, pcB, pc, g.Az);
+                f.wf[c] = wf0 + d;
+                s[6] += (double)d * (double)d;
+            }
         }
     }
     __shared__ double tot[7];
