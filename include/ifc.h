@@ -227,7 +227,10 @@ typedef struct ifc_energy_result {
  * Neumann faces, temp_bc_type/temp_bc_val), solved by unrelaxed red-black
  * Gauss-Seidel sweeps from the current temperature until the RMS change of
  * a sweep falls below tol times the largest of this solve (FP64 norms), or
- * max_sweeps (tol 0: exactly max_sweeps).  The result is the T field
+ * max_sweeps (tol 0: exactly max_sweeps).  With a convection_scheme other
+ * than IFC_CONV_UPWIND the sweeps run in cycles of 25, each starting from the
+ * source plus the deferred correction of the current temperature, and the
+ * solve ends when a cycle meets tol in its first sweep.  The result is the T field
  * (IFC_FIELD_T, written by ifc_write_vtk).  Returns IFC_NOT_CONVERGED when
  * max_sweeps ran out first.  The reference carries TempBCs and writes T but
  * never solves the energy equation. */

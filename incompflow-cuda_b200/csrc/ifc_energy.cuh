@@ -12,6 +12,9 @@
 // wall/inlet form for a Dirichlet face (type 0, the given temperature) and
 // the zero-gradient form for a Neumann face (type 1).  The linear system is
 // solved with the library's red-black Gauss-Seidel sweep kernel, unrelaxed.
+// With a higher-order convection scheme (ifc_convection.cuh) the links stay
+// upwind and the deferred correction of the current temperature is added to
+// the source at the start of every cycle of sweeps (k_temp_dc).
 #pragma once
 
 #include "ifc_kernels.cuh"
@@ -80,5 +83,30 @@ __global__ void k_temp_assemble(Params<T> P, Fields<T> f, TempArgs<T> ta, T *coe
         src[c] = b;
     }
 }
+
+// src_eff = src + the deferred-correction source of the current temperature
+// (same face fluxes and limiter as the momentum equations).
+template <typename T, int DIM>
+__global__ void k_temp_dc(Params<T> P, Fields<T> f, const T *src, T *src_eff)
+{
+    const Geo<T> &g = P.g;
+    const int nx = g.nx, ny = g.ny, pl = nx * ny;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int units = row_units(nx, ny * g.nz);
+    for (int u = gw; u < units; u += nw) {
+        const RowUnit w = row_unit(u, nx, ny);
+        const int c0 = nx * w.r, f0 = (nx + 1) * w.r, v0 = nx * (w.j + (ny + 1) * w.k);
+        for (int i = w.i0 + lane; i < w.i1; i += 32) {
+            const int c = c0 + i;
+            const T wb = DIM == 3 ? f.wf[c] : (T)0, wt = DIM == 3 ? f.wf[c + pl] : (T)0;
+            const T d = dc_cell<T, DIM>(g, f.temp, c, i, w.j, w.k, f.uf[f0 + i], f.uf[f0 + i + 1], f.vf[v0 + i],
+                                        f.vf[v0 + i + nx], wb, wt);
+            src_eff[c] = src[c] + d;
+        }
+    }
+}
+
+static __global__ void k_clear_stop(Ctl *ctl, int eq) { ctl->stop[eq] = 0; }
 
 }  // namespace ifc

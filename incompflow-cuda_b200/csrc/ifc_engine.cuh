@@ -835,17 +835,28 @@ struct Engine : EngineBase {
         if (dim == 2) k_temp_assemble<T, 2><<<grid(N), 256, 0, stream>>>(P, f, ta, f.mc, src);
         else k_temp_assemble<T, 3><<<grid(N), 256, 0, stream>>>(P, f, ta, f.mc, src);
         k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << EQ_W);
+        // Higher-order convection: every cycle of up to 25 sweeps starts from
+        // src + the deferred correction of the current temperature; the solve
+        // has converged when a cycle meets the tolerance in its first sweep.
+        const bool dc = g.conv != CONV_UPWIND;
+        T *src_eff = dc ? f.tmp + N : src;
         SweepArgs<T, 1> A;
         A.coef = f.mc;
         A.phi[0] = f.temp;
         A.old[0] = f.temp;
-        A.src[0] = src;
+        A.src[0] = src_eff;
         A.eq[0] = EQ_W;
         A.active[0] = 1;
         const long long half = (long long)((g.nx + 1) / 2) * g.ny * g.nz;
-        int done = 0;
+        int done = 0, cycle_start = 0;
         while (done < max_sweeps) {
             const int chunk = max_sweeps - done < 25 ? max_sweeps - done : 25;
+            if (dc) {
+                if (dim == 2) k_temp_dc<T, 2><<<row_grid(), 256, 0, stream>>>(P, f, src, src_eff);
+                else k_temp_dc<T, 3><<<row_grid(), 256, 0, stream>>>(P, f, src, src_eff);
+                k_clear_stop<<<1, 1, 0, stream>>>(ctl, EQ_W);
+                cycle_start = done == 0 ? 0 : ctl_h.sweeps[EQ_W];  // host copy read after the last cycle
+            }
             for (int q = 0; q < chunk; ++q)
                 for (int color = 0; color < 2; ++color) {
                     A.color = color;
@@ -856,7 +867,7 @@ struct Engine : EngineBase {
             IFC_CK(cudaGetLastError());
             int rc = read_ctl();
             if (rc != IFC_OK) return rc;
-            if (ctl_h.stop[EQ_W]) break;
+            if (ctl_h.stop[EQ_W] && (!dc || ctl_h.sweeps[EQ_W] - cycle_start <= 1)) break;
         }
         IFC_CK(cudaEventRecord(ev1, stream));
         int rc = read_ctl();
