@@ -117,6 +117,8 @@ struct Engine : EngineBase {
     int spp_mom = 5, spp_p = 5;       // sweeps per pass of the fused kernels
     int spp_persist = 5;              // sweeps per pass of the single-launch solve
     bool persist = false;             // the whole loop runs as one cooperative launch
+    bool persist_mt = false;          // ... with several tiles per CTA
+    int persist_grid = 0;             // CTAs of that launch
     GridBarrier *barrier = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;

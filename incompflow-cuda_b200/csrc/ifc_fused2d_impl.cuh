@@ -164,13 +164,16 @@ void Engine<T>::enq_fused_rc()
 namespace ifc {
 
 // ---- the persistent single-launch 2D solve (ifc_persist2d.cuh) ----
-template <typename T, int KS>
+// launch = false: set the kernel's shared-memory limit and return in *capacity
+// the CTAs that can be co-resident.  launch = true: launch it on e.persist_grid
+// CTAs (e.persist_mt: several tiles per CTA).
+template <typename T, int KS, bool MT>
 static int persist_kernel(Engine<T> &e, bool launch, int *capacity)
 {
     using S = TileShape2D<T>;
     using R = Region<S::TX, S::TY, 2 * KS>;
     const size_t smem = (size_t)3 * R::NR * sizeof(T);
-    auto kern = k_simple2d<T, S::TX, S::TY, KS, S::NT>;
+    auto kern = k_simple2d<T, S::TX, S::TY, KS, S::NT, MT>;
     if (!launch) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return IFC_CUDA_ERROR;
@@ -180,7 +183,6 @@ static int persist_kernel(Engine<T> &e, bool launch, int *capacity)
         *capacity = per_sm * e.nsm;
         return IFC_OK;
     }
-    const int tiles = ((e.P.g.nx + S::TX - 1) / S::TX) * ((e.P.g.ny + S::TY - 1) / S::TY);
     PersistArgs pa;
     pa.n_iter[0] = e.cfg.n_iter_u;
     pa.n_iter[1] = e.cfg.n_iter_v;
@@ -190,24 +192,31 @@ static int persist_kernel(Engine<T> &e, bool launch, int *capacity)
     const char *stall = std::getenv("IFC_TEST_STALL_BARRIER");
     pa.stall_test = (stall && stall[0] == '1') ? 1 : 0;
     void *args[] = {&e.P, &e.f, &e.ctl, &e.partials, &e.barrier, &pa};
-    return cudaLaunchCooperativeKernel((const void *)kern, dim3(tiles), dim3(S::NT), args, smem, e.stream) ==
+    return cudaLaunchCooperativeKernel((const void *)kern, dim3(e.persist_grid), dim3(S::NT), args, smem, e.stream) ==
                    cudaSuccess
                ? IFC_OK
                : IFC_CUDA_ERROR;
 }
 
-template <typename T>
-static int persist_dispatch(Engine<T> &e, int ks, bool launch, int *capacity)
+template <typename T, bool MT>
+static int persist_dispatch_t(Engine<T> &e, int ks, bool launch, int *capacity)
 {
     switch (ks) {
-    case 2: return persist_kernel<T, 2>(e, launch, capacity);
-    case 3: return persist_kernel<T, 3>(e, launch, capacity);
-    case 4: return persist_kernel<T, 4>(e, launch, capacity);
-    case 5: return persist_kernel<T, 5>(e, launch, capacity);
-    case 6: return persist_kernel<T, 6>(e, launch, capacity);
-    case 8: return persist_kernel<T, 8>(e, launch, capacity);
-    default: return persist_kernel<T, 10>(e, launch, capacity);
+    case 2: return persist_kernel<T, 2, MT>(e, launch, capacity);
+    case 3: return persist_kernel<T, 3, MT>(e, launch, capacity);
+    case 4: return persist_kernel<T, 4, MT>(e, launch, capacity);
+    case 5: return persist_kernel<T, 5, MT>(e, launch, capacity);
+    case 6: return persist_kernel<T, 6, MT>(e, launch, capacity);
+    case 8: return persist_kernel<T, 8, MT>(e, launch, capacity);
+    default: return persist_kernel<T, 10, MT>(e, launch, capacity);
     }
+}
+
+template <typename T>
+static int persist_dispatch(Engine<T> &e, int ks, bool launch, int *capacity, bool mt)
+{
+    return mt ? persist_dispatch_t<T, true>(e, ks, launch, capacity)
+              : persist_dispatch_t<T, false>(e, ks, launch, capacity);
 }
 
 static inline int persist_ks(int want)
@@ -217,24 +226,47 @@ static inline int persist_ks(int want)
     return want < 2 ? 2 : (want > 6 ? 6 : want);
 }
 
-// Whether the whole loop fits one cooperative launch (one tile per CTA, all
-// CTAs co-resident).
+// The whole 2D loop as one cooperative launch: one tile per CTA when all tiles'
+// CTAs can be co-resident, otherwise (MT) every CTA visits ceil(tiles / CTAs)
+// tiles in turn, on the fewest CTAs that give that count (so every CTA has the
+// same number of tiles but the last ones).  IFC_PERSIST_OFF=1 keeps the multi-kernel graph; IFC_PERSIST_MAX_CTAS caps the CTAs
+// (used by the tests to run the multi-tile form on small grids).
 template <typename T>
 int Engine<T>::prepare_persist()
 {
     persist = false;
+    persist_mt = false;
     if (dim != 2 || !fused || cfg.linear_solver != IFC_GAUSS_SEIDEL) return IFC_OK;
+    const char *off = std::getenv("IFC_PERSIST_OFF");  // the multi-kernel graph instead (A/B timing, tests)
+    if (off && off[0] == '1') return IFC_OK;
     int coop = 0, dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return IFC_OK;
-    int capacity = 0;
-    if (persist_dispatch<T>(*this, persist_ks(spp_persist), false, &capacity) != IFC_OK) {
+    const int ks = persist_ks(spp_persist);
+    int capacity = 0, capacity_mt = 0;
+    if (persist_dispatch<T>(*this, ks, false, &capacity, false) != IFC_OK ||
+        persist_dispatch<T>(*this, ks, false, &capacity_mt, true) != IFC_OK) {
         cudaGetLastError();
         return IFC_OK;
     }
+    if (const char *cap = std::getenv("IFC_PERSIST_MAX_CTAS")) {
+        const int c = std::atoi(cap);
+        if (c > 0) {
+            capacity = capacity < c ? capacity : c;
+            capacity_mt = capacity_mt < c ? capacity_mt : c;
+        }
+    }
     using S = TileShape2D<T>;
     const int tiles = ((P.g.nx + S::TX - 1) / S::TX) * ((P.g.ny + S::TY - 1) / S::TY);
-    persist = tiles <= capacity;
+    if (tiles <= capacity) {
+        persist = true;
+        persist_grid = tiles;
+    } else if (capacity_mt > 0) {
+        const int per = (tiles + capacity_mt - 1) / capacity_mt;
+        persist = true;
+        persist_mt = true;
+        persist_grid = (tiles + per - 1) / per;
+    }
     return IFC_OK;
 }
 
@@ -243,7 +275,7 @@ int Engine<T>::launch_persist()
 {
     if (cudaMemsetAsync(barrier, 0, sizeof(GridBarrier), stream) != cudaSuccess) return IFC_CUDA_ERROR;
     ++launches;
-    return persist_dispatch<T>(*this, persist_ks(spp_persist), true, nullptr);
+    return persist_dispatch<T>(*this, persist_ks(spp_persist), true, nullptr, persist_mt);
 }
 
 }  // namespace ifc

@@ -1,7 +1,9 @@
 // ifc_persist2d.cuh -- the whole 2D SIMPLE loop in one cooperative launch.
 //
-// Every CTA owns one TX x TY tile for the whole solve and walks through the
-// phases of each outer iteration (src/Solver.cu:160-289):
+// Every CTA owns one TX x TY tile for the whole solve (MT = false) or, when
+// the grid has more tiles than co-resident CTAs, a fixed set of tiles that it
+// visits in turn inside every phase (MT = true), and walks through the phases
+// of each outer iteration (src/Solver.cu:160-289):
 //   momentum passes (assembly + KS red-black sweeps of u and v, temporally
 //   blocked in shared memory as in ifc_fused2d.cuh), Rhie-Chow faces + p'
 //   source, p' passes, [p' mean removal], corrections + convergence test,
@@ -173,7 +175,45 @@ __device__ __forceinline__ void pass_count(LoopState &L, int e, int ns, int N)
     L.cell_updates += (long long)ns * N;
 }
 
-template <typename T, int TX, int TY, int KS, int NT>
+// Origin of tile t (tiles numbered row-major, tiles_x per row) and of its
+// staged region.
+struct Tile {
+    int x0, y0, gx0, gy0;
+};
+
+template <int TX, int TY, int H>
+__device__ __forceinline__ Tile tile_at(int t, int tiles_x)
+{
+    Tile tl;
+    tl.x0 = (t % tiles_x) * TX;
+    tl.y0 = (t / tiles_x) * TY;
+    tl.gx0 = tl.x0 - H;
+    tl.gy0 = tl.y0 - H;
+    return tl;
+}
+
+// This thread's cells of each colour in the staged region of tile tl (cq),
+// their distance from the tile (dq); returns whether the warp owns any tile
+// cell (warps that own none contribute only zeros to the per-sweep sums: they
+// skip the shuffle reduction -- the shuffle unit is shared by the whole SM --
+// and report 0.0, the value the reduction gives).
+template <int W, int H, int TX, int TY, int HH, int NHALF, int NT, int CPT>
+__device__ __forceinline__ bool map_tile(int tid, const Tile &tl, int nx, int ny, int (&cq)[2][CPT], int (&dq)[2][CPT])
+{
+    own_cells<W, HH, NHALF, NT, CPT>(tid, tl.gx0, tl.gy0, nx, ny, cq);
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) dq[c][k] = tile_distance<W, H, TX, TY>(cq[c][k]);
+    bool mine = false;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) mine |= dq[c][k] == 0;
+    return __any_sync(0xffffffffu, mine);
+}
+
+template <typename T, int TX, int TY, int KS, int NT, bool MT>
 __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials,
                                                  GridBarrier *bar, PersistArgs pa)
 {
@@ -186,8 +226,9 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
     const int G = gridDim.x;
     const int tid = threadIdx.x;
     const int tiles_x = (nx + TX - 1) / TX;
-    const int x0 = (blockIdx.x % tiles_x) * TX, y0 = (blockIdx.x / tiles_x) * TY;
-    const int gx0 = x0 - H, gy0 = y0 - H;
+    const int ntiles = tiles_x * ((ny + TY - 1) / TY);
+    // MT: this CTA's tiles are blockIdx.x, blockIdx.x + G, ...; otherwise its
+    // one tile (the tile loops below then have a compile-time trip count of 1).
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *s0 = reinterpret_cast<T *>(smem_raw);
@@ -210,20 +251,8 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         for (int q = 0; q < 8; ++q) L.maxn[q] = ctl->maxn[q];
     }
     int cq[2][CPT], dq[2][CPT];
-    own_cells<W, R::HH, R::NHALF, NT, CPT>(tid, gx0, gy0, nx, ny, cq);
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) dq[c][k] = tile_distance<W, H, TX, TY>(cq[c][k]);
-    // Warps none of whose cells lie in the tile contribute only zeros to the
-    // per-sweep sums; they skip the shuffle reduction (the shuffle unit is
-    // shared by the whole SM) and report 0.0, the value the reduction gives.
-    bool mine = false;
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) mine |= dq[c][k] == 0;
-    const bool wsum = __any_sync(0xffffffffu, mine);
+    const Tile tile0 = tile_at<TX, TY, H>(blockIdx.x, tiles_x);
+    bool wsum = map_tile<W, H, TX, TY, R::HH, R::NHALF, NT, CPT>(tid, tile0, nx, ny, cq, dq);
     __syncthreads();
 
     const int npass_m = (max(pa.n_iter[0], pa.n_iter[1]) + KS - 1) / KS;
@@ -254,12 +283,15 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         // fields at the start of the outer iteration; the momentum passes read
         // them for their halos too, so a barrier follows ----
         if (g.conv != CONV_UPWIND) {
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i >= nx || j >= ny) continue;
-                const int c = i + nx * j;
-                f.sdc[c] = dc_cell<T, 2>(P, f, f.u, i, j, 0);
-                f.sdc[N + c] = dc_cell<T, 2>(P, f, f.v, i, j, 0);
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
+                    if (i >= nx || j >= ny) continue;
+                    const int c = i + nx * j;
+                    f.sdc[c] = dc_cell<T, 2>(P, f, f.u, i, j, 0);
+                    f.sdc[N + c] = dc_cell<T, 2>(P, f, f.v, i, j, 0);
+                }
             }
             if (!grid_sync(bar, G, epoch)) { failed = true; break; }
         }
@@ -270,99 +302,111 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
             const bool au = ns[0] > 0 && !L.stop[EQ_U];
             const bool av = ns[1] > 0 && !L.stop[EQ_V];
             if (!au && !av && pass > 0) continue;
-            for (int q = tid; q < NR; q += NT) {
-                const int a = q % W, b = q / W;
-                const int gi = gx0 + a, gj = gy0 + b;
-                const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
-                const int id = gi + nx * gj;
-                s0[q] = in ? bu[mcur][id] : (T)0;
-                s1[q] = in ? bv[mcur][id] : (T)0;
-                s2[q] = in ? f.p[id] : (T)0;
-            }
-            __syncthreads();
             // The sums of a phase's last pass are never reduced.
             const bool last = pass >= npass_m - 1;
-            T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cbu[2][CPT], cbv[2][CPT];
-            bool own[2][CPT];
-#pragma unroll
-            for (int c = 0; c < 2; ++c)
-#pragma unroll
-                for (int k = 0; k < CPT; ++k) {
-                    const int q = cq[c][k];
-                    own[c][k] = false;
-                    cE[c][k] = cW[c][k] = cN[c][k] = cS[c][k] = cbu[c][k] = cbv[c][k] = (T)0;
-                    cC[c][k] = (T)1;
-                    if (q < 0) continue;
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const bool first = t == (int)blockIdx.x;
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                if (MT) wsum = map_tile<W, H, TX, TY, R::HH, R::NHALF, NT, CPT>(tid, tl, nx, ny, cq, dq);
+                const int gx0 = tl.gx0, gy0 = tl.gy0;
+                for (int q = tid; q < NR; q += NT) {
                     const int a = q % W, b = q / W;
                     const int gi = gx0 + a, gj = gy0 + b;
-                    const int fu = gi + (nx + 1) * gj, fv = gi + nx * gj;
-                    T a7[7], b3[3];
-                    mom_cell<T, 2>(P, gi, gj, 0, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], (T)0, (T)0, s2[q],
-                                   s2[q - 1], s2[q + 1], s2[q - W], s2[q + W], (T)0, (T)0, a7, b3);
-                    add_dc<T, 2>(P, f, fv, b3);
-                    cE[c][k] = a7[AE];
-                    cW[c][k] = a7[AW];
-                    cN[c][k] = a7[AN];
-                    cS[c][k] = a7[AS];
-                    cC[c][k] = a7[AC];
-                    cbu[c][k] = b3[0];
-                    cbv[c][k] = b3[1];
-                    own[c][k] = a >= H && a < H + TX && b >= H && b < H + TY;
+                    const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+                    const int id = gi + nx * gj;
+                    s0[q] = in ? bu[mcur][id] : (T)0;
+                    s1[q] = in ? bv[mcur][id] : (T)0;
+                    s2[q] = in ? f.p[id] : (T)0;
                 }
-            if (pass == 0) {
+                __syncthreads();
+                T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cbu[2][CPT], cbv[2][CPT];
+                bool own[2][CPT];
 #pragma unroll
                 for (int c = 0; c < 2; ++c)
 #pragma unroll
-                    for (int k = 0; k < CPT; ++k)
-                        if (own[c][k]) f.ac[gx0 + cq[c][k] % W + nx * (gy0 + cq[c][k] / W)] = cC[c][k];
-            }
-            const T ru = g.relax[EQ_U], rv = g.relax[EQ_V];
-#pragma unroll 1
-            for (int s = 0; s < KS; ++s) {
-                const bool du = au && s < ns[0];
-                const bool dv = av && s < ns[1];
-                if (!du && !dv) break;
-                double su = 0.0, sv = 0.0;
-#pragma unroll
-                for (int color = 0; color < 2; ++color) {
-                    const int hs = 2 * s + color;
-#pragma unroll
                     for (int k = 0; k < CPT; ++k) {
-                        const int q = cq[color][k];
+                        const int q = cq[c][k];
+                        own[c][k] = false;
+                        cE[c][k] = cW[c][k] = cN[c][k] = cS[c][k] = cbu[c][k] = cbv[c][k] = (T)0;
+                        cC[c][k] = (T)1;
                         if (q < 0) continue;
-                        T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
-                        T d;
-                        if (du && dq[color][k] <= 2 * ns[0] - 1 - hs) {
-                            s0[q] = point_update<T, 2>(a7, cbu[color][k], s0[q], s0[q + 1], s0[q - 1], s0[q + W],
-                                                       s0[q - W], (T)0, (T)0, ru, d);
-                            if (!last && own[color][k]) su += (double)d * (double)d;
-                        }
-                        if (dv && dq[color][k] <= 2 * ns[1] - 1 - hs) {
-                            s1[q] = point_update<T, 2>(a7, cbv[color][k], s1[q], s1[q + 1], s1[q - 1], s1[q + W],
-                                                       s1[q - W], (T)0, (T)0, rv, d);
-                            if (!last && own[color][k]) sv += (double)d * (double)d;
-                        }
+                        const int a = q % W, b = q / W;
+                        const int gi = gx0 + a, gj = gy0 + b;
+                        const int fu = gi + (nx + 1) * gj, fv = gi + nx * gj;
+                        T a7[7], b3[3];
+                        mom_cell<T, 2>(P, gi, gj, 0, f.uf[fu], f.uf[fu + 1], f.vf[fv], f.vf[fv + nx], (T)0, (T)0, s2[q],
+                                       s2[q - 1], s2[q + 1], s2[q - W], s2[q + W], (T)0, (T)0, a7, b3);
+                        add_dc<T, 2>(P, f, fv, b3);
+                        cE[c][k] = a7[AE];
+                        cW[c][k] = a7[AW];
+                        cN[c][k] = a7[AN];
+                        cS[c][k] = a7[AS];
+                        cC[c][k] = a7[AC];
+                        cbu[c][k] = b3[0];
+                        cbv[c][k] = b3[1];
+                        own[c][k] = a >= H && a < H + TX && b >= H && b < H + TY;
                     }
-                    __syncthreads();
+                if (pass == 0) {
+#pragma unroll
+                    for (int c = 0; c < 2; ++c)
+#pragma unroll
+                        for (int k = 0; k < CPT; ++k)
+                            if (own[c][k]) f.ac[gx0 + cq[c][k] % W + nx * (gy0 + cq[c][k] / W)] = cC[c][k];
                 }
-                if (!last) {
-                    if (wsum) {
-                        su = warp_sum(su);
-                        sv = warp_sum(sv);
+                const T ru = g.relax[EQ_U], rv = g.relax[EQ_V];
+#pragma unroll 1
+                for (int s = 0; s < KS; ++s) {
+                    const bool du = au && s < ns[0];
+                    const bool dv = av && s < ns[1];
+                    if (!du && !dv) break;
+                    double su = 0.0, sv = 0.0;
+#pragma unroll
+                    for (int color = 0; color < 2; ++color) {
+                        const int hs = 2 * s + color;
+#pragma unroll
+                        for (int k = 0; k < CPT; ++k) {
+                            const int q = cq[color][k];
+                            if (q < 0) continue;
+                            T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
+                            T d;
+                            if (du && dq[color][k] <= 2 * ns[0] - 1 - hs) {
+                                s0[q] = point_update<T, 2>(a7, cbu[color][k], s0[q], s0[q + 1], s0[q - 1], s0[q + W],
+                                                           s0[q - W], (T)0, (T)0, ru, d);
+                                if (!last && own[color][k]) su += (double)d * (double)d;
+                            }
+                            if (dv && dq[color][k] <= 2 * ns[1] - 1 - hs) {
+                                s1[q] = point_update<T, 2>(a7, cbv[color][k], s1[q], s1[q + 1], s1[q - 1], s1[q + W],
+                                                           s1[q - W], (T)0, (T)0, rv, d);
+                                if (!last && own[color][k]) sv += (double)d * (double)d;
+                            }
+                        }
+                        __syncthreads();
                     }
-                    if ((tid & 31) == 0) {
-                        wred[tid >> 5][s] = su;
-                        wred[tid >> 5][KS + s] = sv;
+                    if (!last) {
+                        if (wsum) {
+                            su = warp_sum(su);
+                            sv = warp_sum(sv);
+                        }
+                        if ((tid & 31) == 0) {
+                            if (MT && !first) {
+                                wred[tid >> 5][s] += su;
+                                wred[tid >> 5][KS + s] += sv;
+                            } else {
+                                wred[tid >> 5][s] = su;
+                                wred[tid >> 5][KS + s] = sv;
+                            }
+                        }
                     }
                 }
-            }
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int a = H + q % TX, b = H + q / TX;
-                const int gi = gx0 + a, gj = gy0 + b;
-                if (gi >= nx || gj >= ny) continue;
-                const int id = gi + nx * gj;
-                bu[mcur ^ 1][id] = s0[b * W + a];
-                bv[mcur ^ 1][id] = s1[b * W + a];
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int a = H + q % TX, b = H + q / TX;
+                    const int gi = gx0 + a, gj = gy0 + b;
+                    if (gi >= nx || gj >= ny) continue;
+                    const int id = gi + nx * gj;
+                    bu[mcur ^ 1][id] = s0[b * W + a];
+                    bv[mcur ^ 1][id] = s1[b * W + a];
+                }
+                if (MT) __syncthreads();  // the next tile's staging overwrites the region
             }
             mcur ^= 1;
             if (!last) block_partials<2 * KS, 2 * KS, NT>(&wred[0][0], partials, G);
@@ -388,21 +432,24 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         fc.v = bv[mcur];
         {
             double m[1] = {0.0};
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i >= nx || j >= ny) continue;
-                const int c = i + nx * j;
-                const T uw = i == 0 ? face_bc(g, WEST, 0, fc.u[c], j) : rc_x(P, fc, i, j);
-                const T ue = i == nx - 1 ? face_bc(g, EAST, 0, fc.u[c], j) : rc_x(P, fc, i + 1, j);
-                const T vs = j == 0 ? face_bc(g, SOUTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j);
-                const T vn = j == ny - 1 ? face_bc(g, NORTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j + 1);
-                const T b = mass_imbalance<T, 2>(g, uw, ue, vs, vn, (T)0, (T)0);
-                f.uf[i + (nx + 1) * j] = uw;
-                if (i == nx - 1) f.uf[nx + (nx + 1) * j] = ue;
-                f.vf[c] = vs;
-                if (j == ny - 1) f.vf[c + nx] = vn;
-                f.sp[c] = b;
-                m[0] += (double)b * (double)b;
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
+                    if (i >= nx || j >= ny) continue;
+                    const int c = i + nx * j;
+                    const T uw = i == 0 ? face_bc(g, WEST, 0, fc.u[c], j) : rc_x(P, fc, i, j);
+                    const T ue = i == nx - 1 ? face_bc(g, EAST, 0, fc.u[c], j) : rc_x(P, fc, i + 1, j);
+                    const T vs = j == 0 ? face_bc(g, SOUTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j);
+                    const T vn = j == ny - 1 ? face_bc(g, NORTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j + 1);
+                    const T b = mass_imbalance<T, 2>(g, uw, ue, vs, vn, (T)0, (T)0);
+                    f.uf[i + (nx + 1) * j] = uw;
+                    if (i == nx - 1) f.uf[nx + (nx + 1) * j] = ue;
+                    f.vf[c] = vs;
+                    if (j == ny - 1) f.vf[c + nx] = vn;
+                    f.sp[c] = b;
+                    m[0] += (double)b * (double)b;
+                }
             }
             write_partials<1, NT>(m, partials + 15 * (size_t)G, G);
             if (!grid_sync(bar, G, epoch)) break;
@@ -412,72 +459,82 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         for (int pass = 0; pass < npass_p; ++pass) {
             const int ns = clamp_sweeps(pa.n_iter[3], pass, KS);
             if (ns <= 0 || L.stop[EQ_P]) continue;
-            for (int q = tid; q < NR; q += NT) {
-                const int a = q % W, b = q / W;
-                const int gi = gx0 + a, gj = gy0 + b;
-                const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
-                const int id = gi + nx * gj;
-                s0[q] = (in && pass > 0) ? bp[pcur][id] : (T)0;
-                s1[q] = in ? (T)1 / f.ac[id] : (T)0;
-            }
-            __syncthreads();
             const bool last = pass == npass_p - 1;
-            T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cb[2][CPT];
-            bool own[2][CPT];
-#pragma unroll
-            for (int c = 0; c < 2; ++c)
-#pragma unroll
-                for (int k = 0; k < CPT; ++k) {
-                    const int q = cq[c][k];
-                    own[c][k] = false;
-                    cE[c][k] = cW[c][k] = cN[c][k] = cS[c][k] = cb[c][k] = (T)0;
-                    cC[c][k] = (T)1;
-                    if (q < 0) continue;
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const bool first = t == (int)blockIdx.x;
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                if (MT) wsum = map_tile<W, H, TX, TY, R::HH, R::NHALF, NT, CPT>(tid, tl, nx, ny, cq, dq);
+                const int gx0 = tl.gx0, gy0 = tl.gy0;
+                for (int q = tid; q < NR; q += NT) {
                     const int a = q % W, b = q / W;
                     const int gi = gx0 + a, gj = gy0 + b;
-                    const T r = s1[q];
-                    const T e = gi < nx - 1 ? (T)(P.d.Kx * (double)(T)(r + s1[q + 1])) : (T)0;
-                    const T w = gi > 0 ? (T)(P.d.Kx * (double)(T)(r + s1[q - 1])) : (T)0;
-                    const T n = gj < ny - 1 ? (T)(P.d.Ky * (double)(T)(r + s1[q + W])) : (T)0;
-                    const T so = gj > 0 ? (T)(P.d.Ky * (double)(T)(r + s1[q - W])) : (T)0;
-                    cE[c][k] = e;
-                    cW[c][k] = w;
-                    cN[c][k] = n;
-                    cS[c][k] = so;
-                    cC[c][k] = -(e + w + n + so);
-                    cb[c][k] = f.sp[gi + nx * gj];
-                    own[c][k] = a >= H && a < H + TX && b >= H && b < H + TY;
+                    const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+                    const int id = gi + nx * gj;
+                    s0[q] = (in && pass > 0) ? bp[pcur][id] : (T)0;
+                    s1[q] = in ? (T)1 / f.ac[id] : (T)0;
                 }
-            const T relax = g.relax[EQ_P];
-#pragma unroll 1
-            for (int s = 0; s < KS; ++s) {
-                if (s >= ns) break;
-                double sx = 0.0;
+                __syncthreads();
+                T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cb[2][CPT];
+                bool own[2][CPT];
 #pragma unroll
-                for (int color = 0; color < 2; ++color) {
-                    const int reach = 2 * ns - 1 - (2 * s + color);
+                for (int c = 0; c < 2; ++c)
 #pragma unroll
                     for (int k = 0; k < CPT; ++k) {
-                        const int q = cq[color][k];
-                        if (q < 0 || dq[color][k] > reach) continue;
-                        T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
-                        T d;
-                        s0[q] = point_update<T, 2>(a7, cb[color][k], s0[q], s0[q + 1], s0[q - 1], s0[q + W],
-                                                   s0[q - W], (T)0, (T)0, relax, d);
-                        if (!last && own[color][k]) sx += (double)d * (double)d;
+                        const int q = cq[c][k];
+                        own[c][k] = false;
+                        cE[c][k] = cW[c][k] = cN[c][k] = cS[c][k] = cb[c][k] = (T)0;
+                        cC[c][k] = (T)1;
+                        if (q < 0) continue;
+                        const int a = q % W, b = q / W;
+                        const int gi = gx0 + a, gj = gy0 + b;
+                        const T r = s1[q];
+                        const T e = gi < nx - 1 ? (T)(P.d.Kx * (double)(T)(r + s1[q + 1])) : (T)0;
+                        const T w = gi > 0 ? (T)(P.d.Kx * (double)(T)(r + s1[q - 1])) : (T)0;
+                        const T n = gj < ny - 1 ? (T)(P.d.Ky * (double)(T)(r + s1[q + W])) : (T)0;
+                        const T so = gj > 0 ? (T)(P.d.Ky * (double)(T)(r + s1[q - W])) : (T)0;
+                        cE[c][k] = e;
+                        cW[c][k] = w;
+                        cN[c][k] = n;
+                        cS[c][k] = so;
+                        cC[c][k] = -(e + w + n + so);
+                        cb[c][k] = f.sp[gi + nx * gj];
+                        own[c][k] = a >= H && a < H + TX && b >= H && b < H + TY;
                     }
-                    __syncthreads();
+                const T relax = g.relax[EQ_P];
+#pragma unroll 1
+                for (int s = 0; s < KS; ++s) {
+                    if (s >= ns) break;
+                    double sx = 0.0;
+#pragma unroll
+                    for (int color = 0; color < 2; ++color) {
+                        const int reach = 2 * ns - 1 - (2 * s + color);
+#pragma unroll
+                        for (int k = 0; k < CPT; ++k) {
+                            const int q = cq[color][k];
+                            if (q < 0 || dq[color][k] > reach) continue;
+                            T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
+                            T d;
+                            s0[q] = point_update<T, 2>(a7, cb[color][k], s0[q], s0[q + 1], s0[q - 1], s0[q + W],
+                                                       s0[q - W], (T)0, (T)0, relax, d);
+                            if (!last && own[color][k]) sx += (double)d * (double)d;
+                        }
+                        __syncthreads();
+                    }
+                    if (!last) {
+                        if (wsum) sx = warp_sum(sx);
+                        if ((tid & 31) == 0) {
+                            if (MT && !first) wred[tid >> 5][s] += sx;
+                            else wred[tid >> 5][s] = sx;
+                        }
+                    }
                 }
-                if (!last) {
-                    if (wsum) sx = warp_sum(sx);
-                    if ((tid & 31) == 0) wred[tid >> 5][s] = sx;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int a = H + q % TX, b = H + q / TX;
+                    const int gi = gx0 + a, gj = gy0 + b;
+                    if (gi >= nx || gj >= ny) continue;
+                    bp[pcur ^ 1][gi + nx * gj] = s0[b * W + a];
                 }
-            }
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int a = H + q % TX, b = H + q / TX;
-                const int gi = gx0 + a, gj = gy0 + b;
-                if (gi >= nx || gj >= ny) continue;
-                bp[pcur ^ 1][gi + nx * gj] = s0[b * W + a];
+                if (MT) __syncthreads();  // the next tile's staging overwrites the region
             }
             pcur ^= 1;
             if (!last) block_partials<KS, 2 * KS, NT>(&wred[0][0], partials, G);
@@ -493,9 +550,12 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
 
         T *const pcc = bp[pcur];  // the current p'
         if (npass_p == 0) {       // no p' sweeps: p' = 0 (src/Solver.cu:193)
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i < nx && j < ny) pcc[i + nx * j] = (T)0;
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
+                    if (i < nx && j < ny) pcc[i + nx * j] = (T)0;
+                }
             }
             if (!grid_sync(bar, G, epoch)) break;
         }
@@ -503,17 +563,23 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         // -------- optional p' mean removal (closed domains, FP64) --------
         if (pa.pin) {
             double m[1] = {0.0};
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i < nx && j < ny) m[0] += (double)pcc[i + nx * j];
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
+                    if (i < nx && j < ny) m[0] += (double)pcc[i + nx * j];
+                }
             }
             write_partials<1, NT>(m, partials, G);
             if (!grid_sync(bar, G, epoch)) break;
             reduce_partials<1, NT>(partials, G, tot);
             const double mean = tot[0] / (double)N;
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i < nx && j < ny) pcc[i + nx * j] = (T)((double)pcc[i + nx * j] - mean);
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
+                    if (i < nx && j < ny) pcc[i + nx * j] = (T)((double)pcc[i + nx * j] - mean);
+                }
             }
             if (!grid_sync(bar, G, epoch)) break;
         }
@@ -521,47 +587,50 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         // ---- corrections + next iteration's boundary faces, kernels.cuh:583-843 ----
         {
             double s[7] = {0, 0, 0, 0, 0, 0, 0};
-            for (int q = tid; q < TX * TY; q += NT) {
-                const int i = x0 + q % TX, j = y0 + q / TX;
-                if (i >= nx || j >= ny) continue;
-                const int c = i + nx * j;
-                const int fu = i + (nx + 1) * j;
-                // loads first
-                const T pc = pcc[c], aC = f.ac[c];
-                const T pcW = i > 0 ? pcc[c - 1] : (T)0, pcE = i < nx - 1 ? pcc[c + 1] : (T)0;
-                const T pcS = j > 0 ? pcc[c - nx] : (T)0, pcN = j < ny - 1 ? pcc[c + nx] : (T)0;
-                const T acW = i > 0 ? f.ac[c - 1] : (T)1, acS = j > 0 ? f.ac[c - nx] : (T)1;
-                const T p0 = f.p[c], u0 = fc.u[c], v0 = fc.v[c];
-                const T uf0 = i > 0 ? f.uf[fu] : (T)0, vf0 = j > 0 ? f.vf[c] : (T)0;
-                const T dp = g.relax[EQ_P] * pc;
-                const T L_ = i > 0 ? pcW : (g.closed[WEST] ? pc : (T)0);
-                const T R_ = i < nx - 1 ? pcE : (g.closed[EAST] ? pc : (T)0);
-                const T du = vel_corr(P.d.ru[0], L_, R_, g.Ax, aC);
-                const T S_ = j > 0 ? pcS : (g.closed[SOUTH] ? pc : (T)0);
-                const T N_ = j < ny - 1 ? pcN : (g.closed[NORTH] ? pc : (T)0);
-                const T dv = vel_corr(P.d.ru[1], S_, N_, g.Ay, aC);
-                const T un = u0 + du, vn = v0 + dv;
-                f.p[c] = p0 + dp;
-                f.u[c] = un;
-                f.v[c] = vn;
-                if (pcc != f.pc) f.pc[c] = pc;  // keep the p' field current for readers
-                s[0] += (double)dp * (double)dp;
-                s[1] += (double)du * (double)du;
-                s[2] += (double)dv * (double)dv;
-                if (i >= 1) {
-                    const T d = face_corr(P.d.ru[0], acW, aC, pcW, pc, g.Ax);
-                    f.uf[fu] = uf0 + d;
-                    s[4] += (double)d * (double)d;
+            for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
+                const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
+                    if (i >= nx || j >= ny) continue;
+                    const int c = i + nx * j;
+                    const int fu = i + (nx + 1) * j;
+                    // loads first
+                    const T pc = pcc[c], aC = f.ac[c];
+                    const T pcW = i > 0 ? pcc[c - 1] : (T)0, pcE = i < nx - 1 ? pcc[c + 1] : (T)0;
+                    const T pcS = j > 0 ? pcc[c - nx] : (T)0, pcN = j < ny - 1 ? pcc[c + nx] : (T)0;
+                    const T acW = i > 0 ? f.ac[c - 1] : (T)1, acS = j > 0 ? f.ac[c - nx] : (T)1;
+                    const T p0 = f.p[c], u0 = fc.u[c], v0 = fc.v[c];
+                    const T uf0 = i > 0 ? f.uf[fu] : (T)0, vf0 = j > 0 ? f.vf[c] : (T)0;
+                    const T dp = g.relax[EQ_P] * pc;
+                    const T L_ = i > 0 ? pcW : (g.closed[WEST] ? pc : (T)0);
+                    const T R_ = i < nx - 1 ? pcE : (g.closed[EAST] ? pc : (T)0);
+                    const T du = vel_corr(P.d.ru[0], L_, R_, g.Ax, aC);
+                    const T S_ = j > 0 ? pcS : (g.closed[SOUTH] ? pc : (T)0);
+                    const T N_ = j < ny - 1 ? pcN : (g.closed[NORTH] ? pc : (T)0);
+                    const T dv = vel_corr(P.d.ru[1], S_, N_, g.Ay, aC);
+                    const T un = u0 + du, vn = v0 + dv;
+                    f.p[c] = p0 + dp;
+                    f.u[c] = un;
+                    f.v[c] = vn;
+                    if (pcc != f.pc) f.pc[c] = pc;  // keep the p' field current for readers
+                    s[0] += (double)dp * (double)dp;
+                    s[1] += (double)du * (double)du;
+                    s[2] += (double)dv * (double)dv;
+                    if (i >= 1) {
+                        const T d = face_corr(P.d.ru[0], acW, aC, pcW, pc, g.Ax);
+                        f.uf[fu] = uf0 + d;
+                        s[4] += (double)d * (double)d;
+                    }
+                    if (j >= 1) {
+                        const T d = face_corr(P.d.ru[1], acS, aC, pcS, pc, g.Ay);
+                        f.vf[c] = vf0 + d;
+                        s[5] += (double)d * (double)d;
+                    }
+                    if (i == 0) f.uf[fu] = face_bc(g, WEST, 0, un, j);
+                    if (i == nx - 1) f.uf[fu + 1] = face_bc(g, EAST, 0, un, j);
+                    if (j == 0) f.vf[c] = face_bc(g, SOUTH, 1, vn, 0);
+                    if (j == ny - 1) f.vf[c + nx] = face_bc(g, NORTH, 1, vn, 0);
                 }
-                if (j >= 1) {
-                    const T d = face_corr(P.d.ru[1], acS, aC, pcS, pc, g.Ay);
-                    f.vf[c] = vf0 + d;
-                    s[5] += (double)d * (double)d;
-                }
-                if (i == 0) f.uf[fu] = face_bc(g, WEST, 0, un, j);
-                if (i == nx - 1) f.uf[fu + 1] = face_bc(g, EAST, 0, un, j);
-                if (j == 0) f.vf[c] = face_bc(g, SOUTH, 1, vn, 0);
-                if (j == ny - 1) f.vf[c + nx] = face_bc(g, NORTH, 1, vn, 0);
             }
             write_partials<7, NT>(s, partials, G);
             if (!grid_sync(bar, G, epoch)) break;
