@@ -266,7 +266,7 @@ struct Engine : EngineBase {
         IFC_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         if (!coop) return IFC_OK;
         const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
-        const size_t per_row = 2 * sizeof(T) * (size_t)nx;
+        const size_t per_row = 2 * sizeof(T) * (size_t)nx + 20;  // p', b_p' and the row table
         const long long max_rows = ((long long)optin - 4096) / (long long)per_row;
         if (max_rows < 1) return IFC_OK;
         long long best = -1, best_per = 0;
@@ -283,7 +283,7 @@ struct Engine : EngineBase {
                 }
             }
         if (best < 0) return IFC_OK;
-        const size_t smem = (size_t)b.bj * b.bk * per_row;
+        const size_t smem = pc3d_smem_bytes<T>(b.bj * b.bk, nx);
         auto kern = k_pc_solve3d<T, kPcNT>;
         IFC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;

@@ -152,6 +152,16 @@ struct PcBlocks {
     int nbj, nbk;  // blocks along j and k
 };
 
+// Dynamic shared memory of k_pc_solve3d for row blocks of `rows` rows of nx
+// cells: per row an int4 (global row offset, j, k, in-block neighbour flags),
+// the list of the block's boundary rows (rounded up to 4 entries), then p'
+// and b_p' of every cell.
+template <typename T>
+__host__ __device__ inline size_t pc3d_smem_bytes(int rows, int nx)
+{
+    return (size_t)rows * 16 + (size_t)((rows + 3) & ~3) * 4 + (size_t)rows * nx * 2 * sizeof(T);
+}
+
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 1) k_pc_solve3d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials,
                                                       GridBarrier *bar, PcBlocks B, int n_sweeps)
@@ -161,18 +171,40 @@ __global__ void __launch_bounds__(NT, 1) k_pc_solve3d(Params<T> P, Fields<T> f, 
     const int G = gridDim.x, tid = threadIdx.x;
     const int j0 = (blockIdx.x % B.nbj) * B.bj, k0 = (blockIdx.x / B.nbj) * B.bk;
     const int nj = min(B.bj, ny - j0), nk = min(B.bk, nz - k0);
-    const int cap = nx * B.bj * B.bk;
+    const int rows_cap = B.bj * B.bk;
+    const int cap = nx * rows_cap;
     const int nrow = nj * nk;
     const int warp = tid >> 5, lane = tid & 31;
     const int ln = nx, lt = nx * nj;  // local strides to the next row in j and in k
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *s_pc = reinterpret_cast<T *>(smem_raw);
+    // Row table (built once per solve, so the sweeps need no integer division
+    // per row): x = global offset of the row, y = j, z = k, w = flags
+    // (1: row j+1 in this block, 2: j-1, 4: k+1, 8: k-1); then the boundary
+    // rows, which every half sweep publishes.
+    int4 *s_row = reinterpret_cast<int4 *>(smem_raw);
+    int *s_bnd = reinterpret_cast<int *>(s_row + rows_cap);
+    T *s_pc = reinterpret_cast<T *>(s_bnd + ((rows_cap + 3) & ~3));
     T *s_sp = s_pc + cap;
+    __shared__ int nbnd;
     T *cC = f.pcoef + (size_t)N * AC, *cE = f.pcoef + (size_t)N * AE;
     T *cN = f.pcoef + (size_t)N * AN, *cT = f.pcoef + (size_t)N * AT;
     __shared__ double red[NT / 32];
     __shared__ double tot2[2];
 
+    for (int r = tid; r < nrow; r += NT) {
+        const int jj = r % nj, kk = r / nj;
+        const int j = j0 + jj, k = k0 + kk;
+        const int fl = (jj + 1 < nj ? 1 : 0) | (jj > 0 ? 2 : 0) | (kk + 1 < nk ? 4 : 0) | (kk > 0 ? 8 : 0);
+        s_row[r] = make_int4(nx * (j + ny * k), j, k, fl);
+    }
+    if (tid == 0) {
+        int n = 0;
+        for (int r = 0; r < nrow; ++r) {
+            const int jj = r % nj, kk = r / nj;
+            if (jj == 0 || jj == nj - 1 || kk == 0 || kk == nk - 1) s_bnd[n++] = r;
+        }
+        nbnd = n;
+    }
     // links of the CTA's cells, b_p', p' = 0
     for (int r = warp; r < nrow; r += NT / 32) {
         const int j = j0 + r % nj, k = k0 + r / nj;
@@ -211,10 +243,10 @@ __global__ void __launch_bounds__(NT, 1) k_pc_solve3d(Params<T> P, Fields<T> f, 
             double sq = 0.0;
             // one warp per row of the block (row r = jj + nj*kk), lanes along x
             for (int r = warp; r < nrow; r += NT / 32) {
-                const int jj = r % nj, kk = r / nj;
-                const int j = j0 + jj, k = k0 + kk;
-                const int lrow = nx * r, crow = nx * (j + ny * k);
-                const bool inN = jj + 1 < nj, inS = jj > 0, inT = kk + 1 < nk, inB = kk > 0;
+                const int4 ri = s_row[r];
+                const int j = ri.y, k = ri.z;
+                const int lrow = nx * r, crow = ri.x;
+                const bool inN = ri.w & 1, inS = ri.w & 2, inT = ri.w & 4, inB = ri.w & 8;
                 for (int i = ((color + j + k) & 1) + 2 * lane; i < nx; i += 64) {
                     const int l = lrow + i, c = crow + i;
                     T a[7];
@@ -239,12 +271,11 @@ __global__ void __launch_bounds__(NT, 1) k_pc_solve3d(Params<T> P, Fields<T> f, 
             }
             __syncthreads();
             // publish this colour's cells of the boundary rows
-            for (int r = warp; r < nrow; r += NT / 32) {
-                const int jj = r % nj, kk = r / nj;
-                if (jj != 0 && jj != nj - 1 && kk != 0 && kk != nk - 1) continue;
-                const int j = j0 + jj, k = k0 + kk;
-                const int lrow = nx * r, crow = nx * (j + ny * k);
-                for (int i = ((color + j + k) & 1) + 2 * lane; i < nx; i += 64) f.pc[crow + i] = s_pc[lrow + i];
+            for (int b = warp; b < nbnd; b += NT / 32) {
+                const int r = s_bnd[b];
+                const int4 ri = s_row[r];
+                const int lrow = nx * r, crow = ri.x;
+                for (int i = ((color + ri.y + ri.z) & 1) + 2 * lane; i < nx; i += 64) f.pc[crow + i] = s_pc[lrow + i];
             }
             // this CTA's sum of the half sweep, in warp order
             sq = warp_sum(sq);
