@@ -124,7 +124,7 @@ __device__ __forceinline__ T dc_cell(const Params<T> &P, const Fields<T> &f, con
 // from the current u, v, w and face velocities; row-segment work units (the
 // six face velocities are read once for the three components).
 template <typename T, int DIM>
-__global__ void k_dc_source(Params<T> P, Fields<T> f)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 3) k_dc_source(Params<T> P, Fields<T> f)
 {
     const Geo<T> &g = P.g;
     const int N = g.N, nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;

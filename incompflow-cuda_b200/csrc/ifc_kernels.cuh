@@ -240,7 +240,7 @@ __global__ void k_copy_active(SweepArgs<T, NC> A, const Ctl *ctl, int N)
 // kernels.cuh:336-500 on interior faces, then :47-95 on boundary faces with the
 // momentum-solve velocities (src/Solver.cu:186-187).
 template <typename T, int DIM>
-__global__ void k_rhie_chow(Params<T> P, Fields<T> f)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 3) k_rhie_chow(Params<T> P, Fields<T> f)
 {
     const Geo<T> &g = P.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
