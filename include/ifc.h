@@ -108,8 +108,8 @@ typedef struct ifc_config {
     int log_level;                    /* 0 silent, 1 reference log cadence on stdout */
     const double *inlet_profile;      /* optional west-face inlet velocity per boundary cell (ny*nz) */
     void *stream;                     /* cudaStream_t to run on, or NULL for a private stream */
-    int convection_scheme;            /* IFC_CONV_* (default IFC_CONV_UPWIND); ifc_batch_solve and
-                                         ifc_adjoint take IFC_CONV_UPWIND only */
+    int convection_scheme;            /* IFC_CONV_* (default IFC_CONV_UPWIND); ifc_adjoint takes
+                                         IFC_CONV_UPWIND only */
 } ifc_config;
 
 typedef struct ifc_stats {

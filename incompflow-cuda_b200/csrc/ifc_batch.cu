@@ -55,6 +55,7 @@ template <typename T>
 struct BPools {
     T *u, *v, *p, *pc, *uf, *vf, *ac, *rac, *sp;
     T *le, *ln, *lc;  // p' links of each cell: east, north, diagonal
+    T *sdu, *sdv;     // deferred-correction sources (higher-order convection; null when no case uses it)
 };
 
 struct BQueue {
@@ -201,6 +202,20 @@ __global__ void __cluster_dims__(kCL, 1, 1) __launch_bounds__(kBNT, 4)
                 }
             __syncthreads();
 
+            // ---- deferred-correction sources of a higher-order convection scheme
+            // (ifc_convection.cuh), from the fields at the start of the iteration
+            if (g.conv != CONV_UPWIND) {
+                T *du = pool.sdu + C.off_c, *dv = pool.sdv + C.off_c;
+                for (int j = gw; j < ny; j += TW)
+                    for (int i = lane; i < nx; i += 32) {
+                        const int c = i + nx * j, fu = i + (nx + 1) * j;
+                        const T uw = uf[fu], ue = uf[fu + 1], vs = vf[c], vn = vf[c + nx];
+                        du[c] = dc_cell<T, 2>(g, u, c, i, j, 0, uw, ue, vs, vn, (T)0, (T)0);
+                        dv[c] = dc_cell<T, 2>(g, v, c, i, j, 0, uw, ue, vs, vn, (T)0, (T)0);
+                    }
+                cl.sync();
+            }
+
             // ---- momentum sweeps, coefficients on the fly (kernels.cuh:97-334, 926-1005)
             const int nm = max(C.n_iter[0], C.n_iter[1]);
             for (int s = 0; s < (nm > 0 ? nm : 1); ++s) {
@@ -220,6 +235,10 @@ __global__ void __cluster_dims__(kCL, 1, 1) __launch_bounds__(kBNT, 4)
                                            i > 0 ? p[c - 1] : (T)0, i < nx - 1 ? p[c + 1] : (T)0,
                                            j > 0 ? p[c - nx] : (T)0, j < ny - 1 ? p[c + nx] : (T)0, (T)0, (T)0, a,
                                            b);
+                            if (g.conv != CONV_UPWIND) {
+                                b[0] = b[0] + pool.sdu[C.off_c + c];
+                                b[1] = b[1] + pool.sdv[C.off_c + c];
+                            }
                             if (s == 0) ac[c] = a[AC];
                             T d;
                             if (du) {
@@ -561,6 +580,7 @@ static int autotune(int cls, const ifc_config &rep)
     constexpr int kCopies = 96;
     std::vector<ifc_config> probe(kCopies, rep);
     for (ifc_config &c : probe) {
+        c.convection_scheme = IFC_CONV_UPWIND;  // the variants differ in their sweeps only
         c.tol_u = c.tol_v = c.tol_w = c.tol_p = 0.0;
         c.tol_mass = 0.0;
         c.num_outer_iter = 20;
@@ -637,7 +657,9 @@ static int batch_run(const ifc_config *cfgs, int n, int force_variant, ifc_batch
         for (int f = 0; f < 4; ++f) closed = closed && cfgs[c].vel_bc_type[f] != IFC_OUTLET;
         b.pin = cfgs[c].pin_pressure == 1 || (cfgs[c].pin_pressure < 0 && closed);
         b.max_outer = cfgs[c].num_outer_iter;
-        if (force_variant >= 0) {
+        if (cfgs[c].convection_scheme != IFC_CONV_UPWIND) {
+            variant[c] = 0;  // only the whole-row kernel applies the deferred correction
+        } else if (force_variant >= 0) {
             variant[c] = force_variant;
         } else {
             std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -688,6 +710,12 @@ static int batch_run(const ifc_config *cfgs, int n, int force_variant, ifc_batch
         for (T **a : cell_arrays) {
             BCK(cudaMalloc(a, nc * sizeof(T)));
             BCK(cudaMemset(*a, 0, nc * sizeof(T)));
+        }
+        bool any_dc = false;
+        for (int c = 0; c < n; ++c) any_dc = any_dc || cfgs[c].convection_scheme != IFC_CONV_UPWIND;
+        if (any_dc) {
+            BCK(cudaMalloc(&pool.sdu, nc * sizeof(T)));
+            BCK(cudaMalloc(&pool.sdv, nc * sizeof(T)));
         }
         BCK(cudaMalloc(&pool.uf, nuf * sizeof(T)));
         BCK(cudaMalloc(&pool.vf, nvf * sizeof(T)));
@@ -781,7 +809,7 @@ done:
     if (e1) cudaEventDestroy(e1);
     if (st) cudaStreamDestroy(st);
     T *all[] = {pool.u, pool.v, pool.p, pool.pc, pool.ac, pool.rac, pool.sp, pool.uf, pool.vf,
-                pool.le, pool.ln, pool.lc, tp.tu, tp.tv, tp.tpc};
+                pool.le, pool.ln, pool.lc, tp.tu, tp.tv, tp.tpc, pool.sdu, pool.sdv};
     for (T *a : all)
         if (a) cudaFree(a);
     if (dcases) cudaFree(dcases);
@@ -805,8 +833,7 @@ extern "C" int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result 
     for (int c = 0; c < n; ++c) {
         const int rc = ifc_config_check(&cases[c]);
         if (rc != IFC_OK) return rc;
-        if (cases[c].dim != 2 || cases[c].linear_solver != IFC_GAUSS_SEIDEL || cases[c].precision != prec ||
-            cases[c].convection_scheme != IFC_CONV_UPWIND)
+        if (cases[c].dim != 2 || cases[c].linear_solver != IFC_GAUSS_SEIDEL || cases[c].precision != prec)
             return IFC_UNSUPPORTED;
     }
     try {

@@ -115,3 +115,24 @@ def test_dc_rejected_by_adjoint(gpu_ok):
     with pytest.raises(ifc.IfcError) as e:
         s.adjoint()
     assert e.value.status == ifc.UNSUPPORTED
+
+
+@pytest.mark.parametrize("scheme", ["quick", "van_leer"])
+def test_dc_batch_matches_oracle(gpu_ok, scheme):
+    """The batched solve applies the correction in its whole-row kernel (every
+    case with a higher-order scheme runs there): each case of a mixed batch
+    equals its oracle solve, which checks the inner early exit after every
+    sweep as that kernel does (tolerance: exact)."""
+    cfgs = [dict(ifc.cavity2d(24, ny=20, re=200.0), convection_scheme=scheme),
+            dict(ifc.channel2d(40, 12), convection_scheme=scheme),
+            ifc.cavity2d(16)]
+    res, fields, _ = ifc.batch_solve(cfgs)
+    for c, r, f in zip(cfgs, res, fields):
+        assert r["converged"], r
+        if "convection_scheme" in c:
+            assert r["sweeps_per_pass"] == 1  # the whole-row kernel
+        o = O.Oracle(to_oracle_cfg(dict(c, check_every=r["sweeps_per_pass"])), "f")
+        n, nm = o.solve()
+        assert nm["converged"] and n == r["outer_iterations"], (n, r["outer_iterations"])
+        for k in ("u", "v"):
+            assert_bitwise(f[k], o.field(k), f"batch {scheme} {c['nx']}x{c['ny']} {k}")
