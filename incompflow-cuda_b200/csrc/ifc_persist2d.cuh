@@ -62,18 +62,23 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks, 
         unsigned int old;
         asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(&b->count) : "memory");
         if (old + 1 < target) {
+            // One L2 round trip per poll; the error flag and the clock are
+            // read every 64 polls only, so they stay off the critical path.
+            // A CTA that passes this barrier while another gave up meets the
+            // flag at the next barrier, which the other never reaches.
             const unsigned long long t0 = global_ns();
             unsigned int spins = 0;
             while (ld_acquire(&b->count) < target) {
-                if (*(volatile int *)&b->err) { good = 0; break; }
-                if ((++spins & 63u) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
-                    atomicExch(&b->err, 1);
-                    good = 0;
-                    break;
+                if ((++spins & 63u) == 0) {
+                    if (*(volatile int *)&b->err) { good = 0; break; }
+                    if (global_ns() - t0 > kBarrierTimeoutNs) {
+                        atomicExch(&b->err, 1);
+                        good = 0;
+                        break;
+                    }
                 }
             }
         }
-        if (*(volatile int *)&b->err) good = 0;
         ok = good;
     }
     __syncthreads();
