@@ -437,24 +437,50 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
         fc.v = bv[mcur];
         {
             double m[1] = {0.0};
+            // The tile's (TX+1) x TY x-faces and TX x (TY+1) y-faces, one per
+            // thread, into shared memory (the staged region is free here);
+            // then every cell's mass imbalance from its four faces.  A face on
+            // the tile's east or north edge is also computed by the next
+            // tile, which owns and stores it (same operations, same value).
+            constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);
+            static_assert(NFX + NFY <= 3 * NR, "faces of a tile must fit the staged region");
+            T *s_f = s0;
             for (int t = blockIdx.x, tn = 0; MT ? t < ntiles : tn < 1; t += G, ++tn) {
                 const Tile tl = MT ? tile_at<TX, TY, H>(t, tiles_x) : tile0;
-                for (int q = tid; q < TX * TY; q += NT) {
-                    const int i = tl.x0 + q % TX, j = tl.y0 + q / TX;
-                    if (i >= nx || j >= ny) continue;
-                    const int c = i + nx * j;
-                    const T uw = i == 0 ? face_bc(g, WEST, 0, fc.u[c], j) : rc_x(P, fc, i, j);
-                    const T ue = i == nx - 1 ? face_bc(g, EAST, 0, fc.u[c], j) : rc_x(P, fc, i + 1, j);
-                    const T vs = j == 0 ? face_bc(g, SOUTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j);
-                    const T vn = j == ny - 1 ? face_bc(g, NORTH, 1, fc.v[c], 0) : rc_y(P, fc, i, j + 1);
-                    const T b = mass_imbalance<T, 2>(g, uw, ue, vs, vn, (T)0, (T)0);
-                    f.uf[i + (nx + 1) * j] = uw;
-                    if (i == nx - 1) f.uf[nx + (nx + 1) * j] = ue;
-                    f.vf[c] = vs;
-                    if (j == ny - 1) f.vf[c + nx] = vn;
-                    f.sp[c] = b;
-                    m[0] += (double)b * (double)b;
+                for (int q = tid; q < NFX + NFY; q += NT) {
+                    if (q < NFX) {
+                        const int a = q % (TX + 1), b = q / (TX + 1);
+                        const int i = tl.x0 + a, j = tl.y0 + b;  // face i of row j
+                        if (i > nx || j >= ny) continue;
+                        const int c = i + nx * j;
+                        const T val = i == 0 ? face_bc(g, WEST, 0, fc.u[c], j)
+                                              : (i == nx ? face_bc(g, EAST, 0, fc.u[c - 1], j) : rc_x(P, fc, i, j));
+                        s_f[q] = val;
+                        if (a < TX || i == nx) f.uf[i + (nx + 1) * j] = val;
+                    } else {
+                        const int q2 = q - NFX;
+                        const int a = q2 % TX, b = q2 / TX;
+                        const int i = tl.x0 + a, j = tl.y0 + b;  // face j of column i
+                        if (i >= nx || j > ny) continue;
+                        const int c = i + nx * j;
+                        const T val = j == 0 ? face_bc(g, SOUTH, 1, fc.v[c], 0)
+                                              : (j == ny ? face_bc(g, NORTH, 1, fc.v[c - nx], 0) : rc_y(P, fc, i, j));
+                        s_f[q] = val;
+                        if (b < TY || j == ny) f.vf[c] = val;
+                    }
                 }
+                __syncthreads();
+                for (int q = tid; q < TX * TY; q += NT) {
+                    const int a = q % TX, b = q / TX;
+                    const int i = tl.x0 + a, j = tl.y0 + b;
+                    if (i >= nx || j >= ny) continue;
+                    const T uw = s_f[a + (TX + 1) * b], ue = s_f[a + 1 + (TX + 1) * b];
+                    const T vs = s_f[NFX + a + TX * b], vn = s_f[NFX + a + TX * (b + 1)];
+                    const T bm = mass_imbalance<T, 2>(g, uw, ue, vs, vn, (T)0, (T)0);
+                    f.sp[i + nx * j] = bm;
+                    m[0] += (double)bm * (double)bm;
+                }
+                if (MT) __syncthreads();  // the next tile's faces overwrite s_f
             }
             write_partials<1, NT>(m, partials + 15 * (size_t)G, G);
             if (!grid_sync(bar, G, epoch)) break;
