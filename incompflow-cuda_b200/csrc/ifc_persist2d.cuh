@@ -321,7 +321,9 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                     const int id = gi + nx * gj;
                     s0[q] = in ? bu[mcur][id] : (T)0;
                     s1[q] = in ? bv[mcur][id] : (T)0;
-                    s2[q] = in ? f.p[id] : (T)0;
+                    // p does not change in the momentum passes: with one tile per
+                    // CTA its region stays in s2 after the first pass
+                    if (MT || pass == 0) s2[q] = in ? f.p[id] : (T)0;
                 }
                 __syncthreads();
                 T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cbu[2][CPT], cbv[2][CPT];
@@ -502,7 +504,9 @@ __global__ void __launch_bounds__(NT) k_simple2d(Params<T> P, Fields<T> f, Ctl *
                     const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
                     const int id = gi + nx * gj;
                     s0[q] = (in && pass > 0) ? bp[pcur][id] : (T)0;
-                    s1[q] = in ? (T)1 / f.ac[id] : (T)0;
+                    // 1/aC does not change in the p' passes: with one tile per
+                    // CTA its region stays in s1 after the first pass
+                    if (MT || pass == 0) s1[q] = in ? (T)1 / f.ac[id] : (T)0;
                 }
                 __syncthreads();
                 T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cb[2][CPT];
