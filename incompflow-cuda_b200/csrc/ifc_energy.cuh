@@ -17,7 +17,7 @@
 // the source at the start of every cycle of sweeps (k_temp_dc).
 #pragma once
 
-#include "ifc_kernels.cuh"
+#include "ifc_fused2d.cuh"
 
 namespace ifc {
 
@@ -108,5 +108,101 @@ __global__ void k_temp_dc(Params<T> P, Fields<T> f, const T *src, T *src_eff)
 }
 
 static __global__ void k_clear_stop(Ctl *ctl, int eq) { ctl->stop[eq] = 0; }
+
+// ---- 2D: KS red-black sweeps on stored coefficients in one pass ------------
+// The temporally blocked pass of ifc_fused2d.cuh for a linear system whose
+// coefficient planes (coef[cell + N*slot], slots aC aE aW aN aS) and source
+// are stored: the tile plus a halo of 2*KS cells is staged from x_in, every
+// thread keeps its cells' coefficients in registers, and the tile after KS
+// sweeps goes to x_out (a different buffer, so no tile reads a neighbour's
+// values of the same pass).  Per-sweep FP64 sums of the owned cells feed the
+// inner early-exit rule of equation eq after the pass (finish_sweeps).  Used
+// by the energy solve; the values equal those of per-sweep red-black launches.
+template <typename T, int TX, int TY, int KS, int NT>
+__global__ void __launch_bounds__(NT) k_coef_pass2d(Params<T> P, const T *coef, const T *src, Ctl *ctl,
+                                                    double *partials, int eq, int ns, const T *x_in, T *x_out)
+{
+    constexpr int H = 2 * KS;
+    using R = Region<TX, TY, H>;
+    constexpr int W = R::W, NR = R::NR;
+    constexpr int CPT = (R::NHALF + NT - 1) / NT;
+    const Geo<T> &g = P.g;
+    const bool active = ns > 0 && !ctl->stop[eq];  // same in every block
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sx = reinterpret_cast<T *>(smem_raw);
+
+    const int nx = g.nx, ny = g.ny, N = g.N;
+    const int tiles_x = (nx + TX - 1) / TX;
+    const int x0 = (blockIdx.x % tiles_x) * TX, y0 = (blockIdx.x / tiles_x) * TY;
+    const int gx0 = x0 - H, gy0 = y0 - H;
+    const int tid = threadIdx.x;
+
+    for (int q = tid; q < NR; q += NT) {
+        const int a = q % W, b = q / W;
+        const int gi = gx0 + a, gj = gy0 + b;
+        const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+        sx[q] = in ? x_in[gi + nx * gj] : (T)0;
+    }
+    int cq[2][CPT], dq[2][CPT];
+    own_cells<W, R::HH, R::NHALF, NT, CPT>(tid, gx0, gy0, nx, ny, cq);
+    T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cb[2][CPT];
+    bool own[2][CPT];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int q = cq[c][k];
+            dq[c][k] = tile_distance<W, H, TX, TY>(q);
+            own[c][k] = false;
+            cE[c][k] = cW[c][k] = cN[c][k] = cS[c][k] = cb[c][k] = (T)0;
+            cC[c][k] = (T)1;
+            if (q < 0) continue;
+            const int a = q % W, b = q / W;
+            const int id = gx0 + a + nx * (gy0 + b);
+            cC[c][k] = coef[id + (size_t)N * AC];
+            cE[c][k] = coef[id + (size_t)N * AE];
+            cW[c][k] = coef[id + (size_t)N * AW];
+            cN[c][k] = coef[id + (size_t)N * AN];
+            cS[c][k] = coef[id + (size_t)N * AS];
+            cb[c][k] = src[id];
+            own[c][k] = a >= H && a < H + TX && b >= H && b < H + TY;
+        }
+    __syncthreads();
+
+    double acc[KS];
+#pragma unroll
+    for (int s = 0; s < KS; ++s) acc[s] = 0.0;
+    const T relax = g.relax[eq];
+#pragma unroll
+    for (int s = 0; s < KS; ++s) {
+        if (!active || s >= ns) break;
+#pragma unroll
+        for (int color = 0; color < 2; ++color) {
+            const int reach = 2 * ns - 1 - (2 * s + color);
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int q = cq[color][k];
+                if (q < 0 || dq[color][k] > reach) continue;
+                T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
+                T d;
+                sx[q] = point_update<T, 2>(a7, cb[color][k], sx[q], sx[q + 1], sx[q - 1], sx[q + W], sx[q - W],
+                                           (T)0, (T)0, relax, d);
+                if (own[color][k]) acc[s] += (double)d * (double)d;
+            }
+            __syncthreads();
+        }
+    }
+    for (int q = tid; q < TX * TY; q += NT) {
+        const int a = H + q % TX, b = H + q / TX;
+        const int gi = gx0 + a, gj = gy0 + b;
+        if (gi >= nx || gj >= ny) continue;
+        x_out[gi + nx * gj] = sx[b * W + a];
+    }
+    if (!active) return;  // uniform: the copy above keeps the output buffer current
+
+    __shared__ double tot[KS];
+    if (grid_reduce<KS>(acc, partials, ctl, tot) && tid == 0) finish_sweeps(ctl, eq, tot, ns, N, g.tol[eq]);
+}
 
 }  // namespace ifc

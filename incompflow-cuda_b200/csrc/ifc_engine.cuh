@@ -850,6 +850,14 @@ struct Engine : EngineBase {
         A.eq[0] = EQ_W;
         A.active[0] = 1;
         const long long half = (long long)((g.nx + 1) / 2) * g.ny * g.nz;
+        // 2D: temporally blocked passes of kEnergyKS sweeps on the stored
+        // coefficients (k_coef_pass2d), ping-ponging T with scratch; the
+        // early-exit rule is then applied after each pass, as in the fused
+        // p' passes.  3D: one launch per colour and sweep.
+        const bool blocked = dim == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL;
+        constexpr int kEnergyKS = 5;
+        const int gran = blocked ? kEnergyKS : 1;  // sweeps counted per early-exit check
+        T *tbuf[2] = {f.temp, f.tmp + 2 * N};
         int done = 0, cycle_start = 0;
         while (done < max_sweeps) {
             const int chunk = max_sweeps - done < 25 ? max_sweeps - done : 25;
@@ -859,17 +867,31 @@ struct Engine : EngineBase {
                 k_clear_stop<<<1, 1, 0, stream>>>(ctl, EQ_W);
                 cycle_start = done == 0 ? 0 : ctl_h.sweeps[EQ_W];  // host copy read after the last cycle
             }
-            for (int q = 0; q < chunk; ++q)
-                for (int color = 0; color < 2; ++color) {
-                    A.color = color;
-                    if (dim == 2) k_sweep<T, 2, 1><<<grid(half), 256, 0, stream>>>(PT, A, ctl, partials);
-                    else k_sweep<T, 3, 1><<<grid(half), 256, 0, stream>>>(PT, A, ctl, partials);
+            if (blocked) {
+                using S = TileShape2D<T>;
+                using R = Region<S::TX, S::TY, 2 * kEnergyKS>;
+                const int tiles = ((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
+                int cur = 0;
+                for (int pass = 0; pass * kEnergyKS < chunk; ++pass) {
+                    k_coef_pass2d<T, S::TX, S::TY, kEnergyKS, S::NT><<<tiles, S::NT, R::NR * sizeof(T), stream>>>(
+                        PT, f.mc, src_eff, ctl, partials, EQ_W, clamp_sweeps(chunk, pass, kEnergyKS), tbuf[cur],
+                        tbuf[cur ^ 1]);
+                    cur ^= 1;
                 }
+                if (cur) IFC_CK(cudaMemcpyAsync(f.temp, tbuf[1], (size_t)N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+            } else {
+                for (int q = 0; q < chunk; ++q)
+                    for (int color = 0; color < 2; ++color) {
+                        A.color = color;
+                        if (dim == 2) k_sweep<T, 2, 1><<<grid(half), 256, 0, stream>>>(PT, A, ctl, partials);
+                        else k_sweep<T, 3, 1><<<grid(half), 256, 0, stream>>>(PT, A, ctl, partials);
+                    }
+            }
             done += chunk;
             IFC_CK(cudaGetLastError());
             int rc = read_ctl();
             if (rc != IFC_OK) return rc;
-            if (ctl_h.stop[EQ_W] && (!dc || ctl_h.sweeps[EQ_W] - cycle_start <= 1)) break;
+            if (ctl_h.stop[EQ_W] && (!dc || ctl_h.sweeps[EQ_W] - cycle_start <= gran)) break;
         }
         IFC_CK(cudaEventRecord(ev1, stream));
         int rc = read_ctl();

@@ -60,6 +60,13 @@ __host__ __device__ __forceinline__ int clamp_sweeps(int n, int pass, int ks)
     return r < 0 ? 0 : (r > ks ? ks : r);
 }
 
+// Tile shapes: FP32 tiles are 32 x 16 cells, FP64 tiles 32 x 8 (the staged
+// region of an FP64 tile needs twice the shared memory per cell).
+template <typename T>
+struct TileShape2D {
+    static constexpr int TX = 32, TY = sizeof(T) == 4 ? 16 : 8, NT = sizeof(T) == 4 ? 1024 : 512;
+};
+
 struct PassArgs {
     int ns[3];      // sweeps of each component in this pass
     int first;      // first pass of the solve (writes aC / starts p' from 0)

@@ -12,12 +12,6 @@ struct PassBufs {
     T *out[2];
 };
 
-// Tile shapes: FP32 tiles are 32 x 16 cells, FP64 tiles 32 x 8 (the staged
-// region of an FP64 tile needs twice the shared memory per cell).
-template <typename T>
-struct TileShape2D {
-    static constexpr int TX = 32, TY = sizeof(T) == 4 ? 16 : 8, NT = sizeof(T) == 4 ? 1024 : 512;
-};
 
 template <typename T, int KS>
 static int launch_mom_pass(Engine<T> &e, const PassArgs &pa, const PassBufs<T> &b, bool prepare = false)
