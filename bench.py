@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--form", default="plain", choices=["plain", "adjoint", "precision", "batch", "convergence"],
+    ap.add_argument("--form", default="plain",
+                    choices=["plain", "adjoint", "precision", "batch", "convergence", "energy"],
                     help="plain: the headline throughput line; adjoint: the differentiation form")
     ap.add_argument("--profiles", type=int, default=32, help="adjoint form: seeded inlet profiles")
     ap.add_argument("--fd-profiles", type=int, default=1,
@@ -636,6 +637,94 @@ def run_batch(args):
         print(json.dumps(line), flush=True)
 
 
+ENERGY_SWEEPS = 2000
+
+
+def run_energy(args):
+    """Energy form: the temperature on the developed 512 x 128 channel flow
+    (600 outer iterations from rest), TempBCs of the reference's config.h
+    (293 K south wall, 373 K north wall, zero gradient elsewhere).  A step is
+    one ifc_solve_energy call of ENERGY_SWEEPS unrelaxed red-black sweeps
+    (tol 0: fixed work), continuing from the previous step's T; the metric is
+    temperature cell-updates/s.  e2e uploads T from pinned host memory before
+    and reads it back after every call."""
+    import numpy as np
+    import torch
+
+    import ifc
+
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    cfg = ifc.channel2d(512, 128, TempBC_type=[1, 1, 0, 0, 1, 1], TempBC_val=[0.0, 0.0, 293.0, 373.0, 0.0, 0.0])
+    s = ifc.Solver(cfg)
+    s.iterate(600)
+    N = s.N
+    for _ in range(max(args.warmup, 1)):
+        s.solve_energy(max_sweeps=ENERGY_SWEEPS, tol=0.0)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = []
+    for _ in range(args.steps):
+        r = s.solve_energy(max_sweeps=ENERGY_SWEEPS, tol=0.0)
+        ms.append(r["device_ms"])
+    clk = clocks.stop()
+    # end to end: T from pinned host memory, the solve, T back to the host
+    t_host = torch.from_numpy(s.get("T")).pin_memory()
+    t_back = torch.empty_like(t_host).pin_memory()
+    lib = ifc.load()
+    fid = ifc.FIELDS.index("T")
+    nbytes = N * 4
+    e2e_ms = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        assert lib.ifc_set_field(s._h, fid, C.c_void_p(t_host.data_ptr()), nbytes) == 0
+        s.solve_energy(max_sweeps=ENERGY_SWEEPS, tol=0.0)
+        assert lib.ifc_get_field(s._h, fid, C.c_void_p(t_back.data_ptr()), nbytes) == 0
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    updates = N * ENERGY_SWEEPS
+    value = updates * len(ms) / (sum(ms) * 1e-3)
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_UPDATE_2D * updates / (statistics.mean(ms) * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        # the oracle's numpy restatement of the same sweeps, one core, on the
+        # same coefficients, for a bounded number of sweeps
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        coef, src = O.energy_assemble(cfg, s.get("uf"), s.get("vf"), None, "f")
+        t = s.get("T").copy()
+        t0 = time.perf_counter()
+        nsw = 0
+        while time.perf_counter() - t0 < args.cpu_seconds:
+            t, _ = O.energy_sweeps(cfg, coef, src, t, 20, "f")
+            nsw += 20
+        dt = time.perf_counter() - t0
+        cpu = {"value": N * nsw / dt, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": f"{nsw} red-black sweeps of the same system, numpy restatement (oracle.energy_sweeps), "
+                         f"{dt:.1f} s on one core of {host_cpu()}"}
+    line = {
+        "metric": "temperature cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(ms), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: channel flow from rest, 600 outer iterations",
+        "config": {"workload": "energy_channel2d_512x128", "sweeps_per_step": ENERGY_SWEEPS,
+                   "linear_solver": "red-black Gauss-Seidel, 5 sweeps per blocked pass",
+                   "l2": "not flushed: the 1.6 MB system stays in L2 by design"},
+        "e2e": {"value": updates * len(e2e_ms) / (sum(e2e_ms) * 1e-3), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+        "roofline": {"bound": "hbm", "kernel": "k_coef_pass2d", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": profiled_traffic("k_coef_pass2d"),
+                     "note": "reference-form 32 B per cell-update; the system lives in L2"},
+        "clocks": clk,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    s.close()
+
+
 def run_convergence(args):
     """Time to convergence on the 64^2 lid-driven cavity (Re 100, alpha
     0.7/0.3, GS 5/5/50, tolerance 1e-5, from rest): this library under the
@@ -762,6 +851,8 @@ def main():
         run_batch(args)
     elif args.form == "convergence":
         run_convergence(args)
+    elif args.form == "energy":
+        run_energy(args)
     else:
         run_ours(args)
 
