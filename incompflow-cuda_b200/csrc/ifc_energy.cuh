@@ -17,7 +17,7 @@
 // the source at the start of every cycle of sweeps (k_temp_dc).
 #pragma once
 
-#include "ifc_fused2d.cuh"
+#include "ifc_persist2d.cuh"
 
 namespace ifc {
 
@@ -108,6 +108,145 @@ __global__ void k_temp_dc(Params<T> P, Fields<T> f, const T *src, T *src_eff)
 }
 
 static __global__ void k_clear_stop(Ctl *ctl, int eq) { ctl->stop[eq] = 0; }
+
+// ---- 2D: a cycle of sweeps on stored coefficients in one cooperative launch --
+// The passes of k_coef_pass2d (below) with one tile per CTA, all CTAs
+// co-resident: the coefficients are read into registers once per cycle, the
+// passes are separated by the bounded grid barrier of ifc_persist2d.cuh, and
+// after each pass every CTA reduces the per-sweep FP64 sums (double-buffered
+// by pass parity, so a CTA that runs ahead cannot overwrite sums another is
+// still reading) and applies the inner early-exit rule exactly as
+// finish_sweeps does.  The result is left in x0.  Values equal those of the
+// per-pass launches.
+template <typename T, int TX, int TY, int KS, int NT>
+__global__ void __launch_bounds__(NT) k_coef_solve2d(Params<T> P, const T *coef, const T *src, Ctl *ctl,
+                                                     double *partials, GridBarrier *bar, int eq, int nsweeps, T *x0,
+                                                     T *x1)
+{
+    constexpr int H = 2 * KS;
+    using R = Region<TX, TY, H>;
+    constexpr int W = R::W, NR = R::NR;
+    constexpr int CPT = (R::NHALF + NT - 1) / NT;
+    const Geo<T> &g = P.g;
+    const int nx = g.nx, ny = g.ny, N = g.N, G = gridDim.x;
+    const int tiles_x = (nx + TX - 1) / TX;
+    const int x0t = (blockIdx.x % tiles_x) * TX, y0t = (blockIdx.x / tiles_x) * TY;
+    const int gx0 = x0t - H, gy0 = y0t - H;
+    const int tid = threadIdx.x;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sx = reinterpret_cast<T *>(smem_raw);
+    __shared__ double wred[NT / 32][KS];
+    __shared__ double tot[KS];
+    __shared__ int s_stop;
+
+    int cq[2][CPT], dq[2][CPT];
+    own_cells<W, R::HH, R::NHALF, NT, CPT>(tid, gx0, gy0, nx, ny, cq);
+    T cE[2][CPT], cW[2][CPT], cN[2][CPT], cS[2][CPT], cC[2][CPT], cb[2][CPT];
+    bool own[2][CPT];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int q = cq[c][k];
+            dq[c][k] = tile_distance<W, H, TX, TY>(q);
+            own[c][k] = false;
+            cE[c][k] = cW[c][k] = cN[c][k] = cS[c][k] = cb[c][k] = (T)0;
+            cC[c][k] = (T)1;
+            if (q < 0) continue;
+            const int a = q % W, b = q / W;
+            const int id = gx0 + a + nx * (gy0 + b);
+            cC[c][k] = coef[id + (size_t)N * AC];
+            cE[c][k] = coef[id + (size_t)N * AE];
+            cW[c][k] = coef[id + (size_t)N * AW];
+            cN[c][k] = coef[id + (size_t)N * AN];
+            cS[c][k] = coef[id + (size_t)N * AS];
+            cb[c][k] = src[id];
+            own[c][k] = a >= H && a < H + TX && b >= H && b < H + TY;
+        }
+    double mx = ctl->inner_max[eq];
+    int sw = ctl->sweeps[eq];
+    long long cu = ctl->cell_updates;
+    double last_sq = ctl->last_sweep_sq[eq];
+    if (tid == 0) s_stop = ctl->stop[eq];
+    __syncthreads();
+    bool stop = s_stop != 0;
+    bool failed = false;
+    unsigned int epoch = 0;
+    T *buf[2] = {x0, x1};
+    int cur = 0;
+    const T relax = g.relax[eq];
+
+    for (int pass = 0; pass * KS < nsweeps && !stop; ++pass) {
+        const int ns = clamp_sweeps(nsweeps, pass, KS);
+        for (int q = tid; q < NR; q += NT) {
+            const int a = q % W, b = q / W;
+            const int gi = gx0 + a, gj = gy0 + b;
+            const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+            sx[q] = in ? buf[cur][gi + nx * gj] : (T)0;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int s = 0; s < KS; ++s) {
+            if (s >= ns) break;
+            double acc = 0.0;
+#pragma unroll
+            for (int color = 0; color < 2; ++color) {
+                const int reach = 2 * ns - 1 - (2 * s + color);
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const int q = cq[color][k];
+                    if (q < 0 || dq[color][k] > reach) continue;
+                    T a7[7] = {cC[color][k], cE[color][k], cW[color][k], cN[color][k], cS[color][k], (T)0, (T)0};
+                    T d;
+                    sx[q] = point_update<T, 2>(a7, cb[color][k], sx[q], sx[q + 1], sx[q - 1], sx[q + W], sx[q - W],
+                                               (T)0, (T)0, relax, d);
+                    if (own[color][k]) acc += (double)d * (double)d;
+                }
+                __syncthreads();
+            }
+            acc = warp_sum(acc);
+            if ((tid & 31) == 0) wred[tid >> 5][s] = acc;
+        }
+        for (int q = tid; q < TX * TY; q += NT) {
+            const int a = H + q % TX, b = H + q / TX;
+            const int gi = gx0 + a, gj = gy0 + b;
+            if (gi >= nx || gj >= ny) continue;
+            buf[cur ^ 1][gi + nx * gj] = sx[b * W + a];
+        }
+        cur ^= 1;
+        double *part = partials + (size_t)(pass & 1) * KS * G;
+        block_partials<KS, KS, NT>(&wred[0][0], part, G);
+        if (!grid_sync(bar, G, epoch)) { failed = true; break; }
+        reduce_partials<KS, NT>(part, G, tot);
+        // the rule of finish_sweeps, evaluated identically in every CTA
+        bool stop_now = false;
+        for (int s = 0; s < ns; ++s) {
+            if (stop_now) break;
+            const double rms = sqrt(tot[s] / (double)N);
+            if (rms > mx) mx = rms;
+            if (rms / (mx + 1e-20) < g.tol[eq]) stop_now = true;
+        }
+        sw += ns;
+        cu += (long long)ns * N;
+        last_sq = tot[ns - 1];
+        stop = stop_now;
+        __syncthreads();  // tot is rewritten only after the next pass's barrier
+    }
+    if (!failed && cur == 1)  // the last pass staged from x0, and every CTA has passed its barrier
+        for (int q = tid; q < TX * TY; q += NT) {
+            const int gi = x0t + q % TX, gj = y0t + q / TX;
+            if (gi < nx && gj < ny) x0[gi + nx * gj] = x1[gi + nx * gj];
+        }
+    if (blockIdx.x == 0 && tid == 0 && !failed) {
+        ctl->inner_max[eq] = mx;
+        ctl->sweeps[eq] = sw;
+        ctl->cell_updates = cu;
+        ctl->last_sweep_sq[eq] = last_sq;
+        if (stop) ctl->stop[eq] = 1;
+    }
+    if (tid == 0 && (failed || bar->err)) atomicExch(&ctl->status, 3);
+}
 
 // ---- 2D: KS red-black sweeps on stored coefficients in one pass ------------
 // The temporally blocked pass of ifc_fused2d.cuh for a linear system whose

@@ -858,19 +858,38 @@ struct Engine : EngineBase {
         constexpr int kEnergyKS = 5;
         const int gran = blocked ? kEnergyKS : 1;  // sweeps counted per early-exit check
         T *tbuf[2] = {f.temp, f.tmp + 2 * N};
+        // Cycles of 25 sweeps with a host check between them; without the
+        // deferred correction the cooperative kernel applies the early-exit
+        // rule on the device, so the whole solve is one cycle there.
+        int cycle_len = 25;
+        {
+            using S = TileShape2D<T>;
+            const int tiles = ((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
+            if (blocked && !dc && energy_coop(tiles) && max_sweeps > 0) cycle_len = max_sweeps;
+        }
         int done = 0, cycle_start = 0;
         while (done < max_sweeps) {
-            const int chunk = max_sweeps - done < 25 ? max_sweeps - done : 25;
+            const int chunk = max_sweeps - done < cycle_len ? max_sweeps - done : cycle_len;
             if (dc) {
                 if (dim == 2) k_temp_dc<T, 2><<<row_grid(), 256, 0, stream>>>(P, f, src, src_eff);
                 else k_temp_dc<T, 3><<<row_grid(), 256, 0, stream>>>(P, f, src, src_eff);
                 k_clear_stop<<<1, 1, 0, stream>>>(ctl, EQ_W);
                 cycle_start = done == 0 ? 0 : ctl_h.sweeps[EQ_W];  // host copy read after the last cycle
             }
-            if (blocked) {
-                using S = TileShape2D<T>;
-                using R = Region<S::TX, S::TY, 2 * kEnergyKS>;
-                const int tiles = ((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
+            using S = TileShape2D<T>;
+            using R = Region<S::TX, S::TY, 2 * kEnergyKS>;
+            const int tiles = ((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
+            if (blocked && energy_coop(tiles)) {
+                // the whole cycle in one cooperative launch (k_coef_solve2d)
+                IFC_CK(cudaMemsetAsync(barrier, 0, sizeof(GridBarrier), stream));
+                int ns_cycle = chunk, eq = EQ_W;
+                T *x1 = tbuf[1];
+                const T *coef = f.mc, *srcp = src_eff;
+                void *args[] = {&PT, &coef, &srcp, &ctl, &partials, &barrier, &eq, &ns_cycle, &f.temp, &x1};
+                IFC_CK(cudaLaunchCooperativeKernel((const void *)k_coef_solve2d<T, S::TX, S::TY, kEnergyKS, S::NT>,
+                                                   dim3(tiles), dim3(S::NT), args, R::NR * sizeof(T), stream));
+                ++launches;
+            } else if (blocked) {
                 int cur = 0;
                 for (int pass = 0; pass * kEnergyKS < chunk; ++pass) {
                     k_coef_pass2d<T, S::TX, S::TY, kEnergyKS, S::NT><<<tiles, S::NT, R::NR * sizeof(T), stream>>>(
@@ -910,6 +929,27 @@ struct Engine : EngineBase {
         k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << EQ_W);
         IFC_CK(cudaStreamSynchronize(stream));
         return ctl_h.stop[EQ_W] || tol == 0.0 ? IFC_OK : IFC_NOT_CONVERGED;
+    }
+
+    // Whether the energy cycle fits one cooperative launch (one tile per CTA).
+    int energy_coop_state = -1;
+    bool energy_coop(int tiles)
+    {
+        if (energy_coop_state < 0) {
+            using S = TileShape2D<T>;
+            using R = Region<S::TX, S::TY, 10>;
+            int per_sm = 0, dev = 0, coop = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+            if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coef_solve2d<T, S::TX, S::TY, 5, S::NT>,
+                                                                      S::NT, R::NR * sizeof(T)) != cudaSuccess) {
+                cudaGetLastError();
+                per_sm = 0;
+            }
+            const char *off = std::getenv("IFC_PERSIST_OFF");
+            energy_coop_state = coop && per_sm > 0 && !(off && off[0] == '1') && tiles <= per_sm * nsm ? 1 : 0;
+        }
+        return energy_coop_state == 1;
     }
 
     int set_inlet(const double *profile) override

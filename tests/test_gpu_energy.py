@@ -12,11 +12,22 @@ from helpers import assert_bitwise
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("case", ["cavity24", "channel48x16", "cavity3d8", "cavity24_fp64"])
-def test_energy_sweeps_match_oracle(gpu_ok, case):
+@pytest.fixture(params=["cooperative", "passes"])
+def energy_form(request, monkeypatch):
+    """Both 2D device forms of the energy sweeps: one cooperative launch per
+    cycle, or one launch per pass of 5 sweeps (IFC_PERSIST_OFF=1)."""
+    if request.param == "passes":
+        monkeypatch.setenv("IFC_PERSIST_OFF", "1")
+    else:
+        monkeypatch.delenv("IFC_PERSIST_OFF", raising=False)
+    return request.param
+
+
+@pytest.mark.parametrize("case", ["cavity24", "channel48x16", "cavity3d8", "cavity24_fp64", "channel200x70"])
+def test_energy_sweeps_match_oracle(gpu_ok, energy_form, case):
     prec = "d" if case.endswith("fp64") else "f"
     cfg = {"cavity24": ifc.cavity2d(24), "channel48x16": ifc.channel2d(48, 16), "cavity3d8": ifc.cavity3d(8),
-           "cavity24_fp64": ifc.cavity2d(24)}[case]
+           "cavity24_fp64": ifc.cavity2d(24), "channel200x70": ifc.channel2d(200, 70)}[case]
     cfg = dict(cfg, precision=prec, numOuterIter=400)
     s = ifc.Solver(cfg)
     s.solve()
@@ -45,7 +56,7 @@ def test_energy_converges_within_wall_temperatures(gpu_ok):
 
 @pytest.mark.parametrize("scheme", ["quick", "van_leer"])
 @pytest.mark.parametrize("case", ["channel48x16", "cavity3d8", "cavity24_fp64"])
-def test_energy_dc_cycles_match_oracle(gpu_ok, case, scheme):
+def test_energy_dc_cycles_match_oracle(gpu_ok, energy_form, case, scheme):
     """Higher-order convection of T: every cycle of 25 sweeps starts from the
     source plus the deferred correction of the current T.  With tol 0 the
     cycles are fixed (25, 25, 10) and the device matches the numpy restatement
