@@ -173,6 +173,15 @@ int ifc_write_vtk(ifc_solver *h, const char *path);
 int ifc_write_vtk_host(const ifc_config *cfg, const void *u, const void *v, const void *w,
                        const void *p, const void *temp, const char *path);
 
+/* The same file in legacy VTK BINARY encoding: the header says BINARY and
+ * every data block (coordinates, temperature, velocity, pressure) holds
+ * big-endian values of the handle's scalar type, "float" or "double", so FP64
+ * fields are written without rounding.  No counterpart in the reference, which
+ * writes ASCII only (src/Solver.cu:301-367). */
+int ifc_write_vtk_binary(ifc_solver *h, const char *path);
+int ifc_write_vtk_binary_host(const ifc_config *cfg, const void *u, const void *v, const void *w,
+                              const void *p, const void *temp, const char *path);
+
 /* ---- batched form: many independent 2D cases in one persistent launch ---- */
 typedef struct ifc_batch_result {
     int status;                       /* IFC_OK (converged), IFC_NOT_CONVERGED, IFC_DIVERGED */

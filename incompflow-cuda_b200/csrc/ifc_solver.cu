@@ -302,10 +302,8 @@ int ifc_get_stats(ifc_solver *h, ifc_stats *stats)
     IFC_END(h)
 }
 
-int ifc_write_vtk(ifc_solver *h, const char *path)
+static int write_vtk_any(ifc_solver *h, const char *path, bool binary)
 {
-    NvtxRange r("ifc_write_vtk");
-    if (!path) return IFC_BAD_ARGUMENT;
     IFC_GUARD(h)
     const size_t bytes = h->eng->field_size(IFC_FIELD_U);
     std::vector<char> u(bytes), v(bytes), w(bytes), p(bytes), t(bytes);
@@ -315,8 +313,23 @@ int ifc_write_vtk(ifc_solver *h, const char *path)
     if ((rc = h->eng->get_field(IFC_FIELD_W, w.data(), bytes)) != IFC_OK) return rc;
     if ((rc = h->eng->get_field(IFC_FIELD_P, p.data(), bytes)) != IFC_OK) return rc;
     if ((rc = h->eng->get_field(IFC_FIELD_T, t.data(), bytes)) != IFC_OK) return rc;
-    return ifc_write_vtk_host(&h->cfg, u.data(), v.data(), w.data(), p.data(), t.data(), path);
+    return binary ? ifc_write_vtk_binary_host(&h->cfg, u.data(), v.data(), w.data(), p.data(), t.data(), path)
+                  : ifc_write_vtk_host(&h->cfg, u.data(), v.data(), w.data(), p.data(), t.data(), path);
     IFC_END(h)
+}
+
+int ifc_write_vtk(ifc_solver *h, const char *path)
+{
+    NvtxRange r("ifc_write_vtk");
+    if (!path) return IFC_BAD_ARGUMENT;
+    return write_vtk_any(h, path, false);
+}
+
+int ifc_write_vtk_binary(ifc_solver *h, const char *path)
+{
+    NvtxRange r("ifc_write_vtk_binary");
+    if (!path) return IFC_BAD_ARGUMENT;
+    return write_vtk_any(h, path, true);
 }
 
 const char *ifc_last_error(const ifc_solver *h)

@@ -177,7 +177,90 @@ int write_vtk(const ifc_config *cfg, const T *u, const T *v, const T *w, const T
     return ok ? IFC_OK : IFC_IO_ERROR;
 }
 
+// ---- legacy VTK BINARY ------------------------------------------------------
+// The same file as above with the data blocks in the legacy format's binary
+// encoding: big-endian values of the scalar type ("float" for FP32 handles,
+// "double" for FP64 handles, so nothing is rounded), each block followed by a
+// newline.  Header, coordinates (computed in the scalar type) and FIELD blocks
+// are those of the ASCII file.
+
+template <typename T>
+void put_be(std::vector<unsigned char> &out, T x)
+{
+    unsigned char b[sizeof(T)];
+    std::memcpy(b, &x, sizeof(T));
+    for (int k = (int)sizeof(T) - 1; k >= 0; --k) out.push_back(b[k]);  // the hosts here are little-endian
+}
+
+template <typename T>
+bool write_be_block(FILE *fp, const T *a, const T *b, const T *c, size_t n)
+{
+    std::vector<unsigned char> out;
+    const size_t chunk = 1 << 16;
+    for (size_t lo = 0; lo < n; lo += chunk) {
+        const size_t hi = std::min(n, lo + chunk);
+        out.clear();
+        out.reserve((hi - lo) * sizeof(T) * (c ? 3 : 1));
+        for (size_t q = lo; q < hi; ++q) {
+            put_be(out, a[q]);
+            if (c) {
+                put_be(out, b[q]);
+                put_be(out, c[q]);
+            }
+        }
+        if (std::fwrite(out.data(), 1, out.size(), fp) != out.size()) return false;
+    }
+    return std::fputc('\n', fp) != EOF;
+}
+
+template <typename T>
+int write_vtk_binary(const ifc_config *cfg, const T *u, const T *v, const T *w, const T *p, const T *temp,
+                     const char *path)
+{
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->dim == 2 ? 1 : cfg->nz;
+    const T xmin = (T)cfg->xmin, ymin = (T)cfg->ymin, zmin = (T)cfg->zmin;
+    const T dx = ((T)cfg->xmax - xmin) / (T)nx;
+    const T dy = ((T)cfg->ymax - ymin) / (T)ny;
+    const T dz = ((T)cfg->zmax - zmin) / (T)nz;
+    const char *ty = sizeof(T) == 8 ? "double" : "float";
+    FILE *fp = std::fopen(path, "wb");
+    if (!fp) return IFC_IO_ERROR;
+    const long long ncell = (long long)nx * ny * nz;
+    bool ok = std::fprintf(fp, "# vtk DataFile Version 3.0\nflash 3d grid and solution\nBINARY\n"
+                               "DATASET RECTILINEAR_GRID\n") > 0;
+    ok = ok && std::fprintf(fp, "DIMENSIONS %d %d %d\n", nx + 1, ny + 1, nz + 1) > 0;
+    const struct { const char *name; int n; T lo, d; } ax[3] = {
+        {"X_COORDINATES", nx, xmin, dx}, {"Y_COORDINATES", ny, ymin, dy}, {"Z_COORDINATES", nz, zmin, dz}};
+    for (const auto &A : ax) {
+        ok = ok && std::fprintf(fp, "%s %d %s\n", A.name, A.n + 1, ty) > 0;
+        std::vector<T> x((size_t)A.n + 1);
+        for (int i = 0; i <= A.n; ++i) x[i] = A.lo + (T)i * A.d;
+        ok = ok && write_be_block<T>(fp, x.data(), nullptr, nullptr, x.size());
+    }
+    ok = ok && std::fprintf(fp, "CELL_DATA %lld\nFIELD FieldData 3\n", ncell) > 0;
+    ok = ok && std::fprintf(fp, "temperature 1 %lld %s\n", ncell, ty) > 0;
+    ok = ok && write_be_block<T>(fp, temp, nullptr, nullptr, (size_t)ncell);
+    ok = ok && std::fprintf(fp, "velocity 3 %lld %s\n", ncell, ty) > 0;
+    ok = ok && write_be_block<T>(fp, u, v, w, (size_t)ncell);
+    ok = ok && std::fprintf(fp, "pressure 1 %lld %s\n", ncell, ty) > 0;
+    ok = ok && write_be_block<T>(fp, p, nullptr, nullptr, (size_t)ncell);
+    if (std::fclose(fp) != 0) ok = false;
+    return ok ? IFC_OK : IFC_IO_ERROR;
+}
+
 }  // namespace
+
+extern "C" int ifc_write_vtk_binary_host(const ifc_config *cfg, const void *u, const void *v, const void *w,
+                                         const void *p, const void *temp, const char *path)
+{
+    if (!cfg || !u || !v || !w || !p || !temp || !path) return IFC_BAD_ARGUMENT;
+    if (ifc_config_check(cfg) != IFC_OK) return IFC_BAD_CONFIG;
+    if (cfg->precision == IFC_FP64)
+        return write_vtk_binary<double>(cfg, (const double *)u, (const double *)v, (const double *)w,
+                                        (const double *)p, (const double *)temp, path);
+    return write_vtk_binary<float>(cfg, (const float *)u, (const float *)v, (const float *)w, (const float *)p,
+                                   (const float *)temp, path);
+}
 
 extern "C" int ifc_write_vtk_host(const ifc_config *cfg, const void *u, const void *v, const void *w,
                                   const void *p, const void *temp, const char *path)

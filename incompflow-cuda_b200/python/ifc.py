@@ -120,6 +120,8 @@ EXPORTS = {
     "ifc_iterate": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(IfcStats)]),
     "ifc_write_vtk": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ifc_write_vtk_host": (C.c_int, [C.POINTER(IfcConfig)] + [C.c_void_p] * 5 + [C.c_char_p]),
+    "ifc_write_vtk_binary": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ifc_write_vtk_binary_host": (C.c_int, [C.POINTER(IfcConfig)] + [C.c_void_p] * 5 + [C.c_char_p]),
     "ifc_run_stage": (C.c_int, [C.c_void_p, C.c_int]),
     "ifc_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "ifc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(IfcStats)]),
@@ -352,8 +354,11 @@ class Solver:
         self._check(load().ifc_get_stats(self._h, C.byref(st)), "stats")
         return st.as_dict()
 
-    def write_vtk(self, path: str):
-        self._check(load().ifc_write_vtk(self._h, path.encode()), "write_vtk")
+    def write_vtk(self, path: str, binary: bool = False):
+        """ASCII VTK as the reference writes it, or (binary=True) legacy VTK
+        BINARY with the values of the handle's precision."""
+        fn = load().ifc_write_vtk_binary if binary else load().ifc_write_vtk
+        self._check(fn(self._h, path.encode()), "write_vtk")
 
     def solve_energy(self, max_sweeps: int = 20000, tol: float = 1e-6) -> dict:
         """Steady temperature on the current flow (ifc_solve_energy)."""
@@ -398,12 +403,14 @@ class Solver:
         return outs, dth, dmu.value
 
 
-def write_vtk_host(cfg: dict, u, v, w, p, temp, path: str):
-    """The VTK writer on host arrays (no GPU)."""
+def write_vtk_host(cfg: dict, u, v, w, p, temp, path: str, binary: bool = False):
+    """The VTK writer on host arrays (no GPU); binary=True writes legacy VTK
+    BINARY."""
     s, keep = make_struct(cfg)
     dt = np.float64 if s.precision == 1 else np.float32
     arrs = [np.ascontiguousarray(a, dtype=dt).ravel() for a in (u, v, w, p, temp)]
-    rc = load().ifc_write_vtk_host(C.byref(s), *[a.ctypes.data for a in arrs], path.encode())
+    fn = load().ifc_write_vtk_binary_host if binary else load().ifc_write_vtk_host
+    rc = fn(C.byref(s), *[a.ctypes.data for a in arrs], path.encode())
     if rc != OK:
         raise IfcError(rc, "write_vtk_host")
 

@@ -86,3 +86,75 @@ def test_value_formatting_matches_printf_g(prec, tmp_path):
     ref = ["%g" % float(x) for x in u]
     bad = [i for i in range(u.size) if got[i] != ref[i]]
     assert not bad, [(float(u[i]), got[i], ref[i]) for i in bad[:5]]
+
+
+def read_legacy_binary_vtk(path):
+    """Reads the legacy VTK BINARY layout written by ifc_write_vtk_binary_host:
+    text header lines, then for each block a label line "<name> <count...>
+    <type>" followed by big-endian values and a newline."""
+    data = open(path, "rb").read()
+    pos = 0
+
+    def line():
+        nonlocal pos
+        end = data.index(b"\n", pos)
+        s = data[pos:end].decode()
+        pos = end + 1
+        return s
+
+    def block(count, ty):
+        nonlocal pos
+        dt = np.dtype(">f4" if ty == "float" else ">f8")
+        a = np.frombuffer(data, dtype=dt, count=count, offset=pos).astype(dt.newbyteorder("="))
+        pos += count * dt.itemsize
+        assert data[pos:pos + 1] == b"\n"
+        pos += 1
+        return a
+
+    hdr = [line() for _ in range(5)]
+    out = {"header": hdr}
+    for _ in range(3):
+        name, n, ty = line().split()
+        out[name] = block(int(n), ty)
+    out["cell_data"] = line()
+    out["field"] = line()
+    for _ in range(3):
+        name, comps, n, ty = line().split()
+        out[name] = block(int(comps) * int(n), ty)
+        out[name + "_type"] = ty
+    assert pos == len(data)
+    return out
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+@pytest.mark.parametrize("cfg", [ifc.channel2d(12, 5), ifc.cavity3d(4, nx=4, ny=3, nz=5)])
+def test_vtk_binary_round_trip(tmp_path, cfg, prec):
+    """Every value comes back exactly, in the handle's precision; header and
+    coordinates match the ASCII file's (coordinates to its 6 digits)."""
+    cfg = dict(cfg, precision=prec)
+    dt = np.float32 if prec == "f" else np.float64
+    nx, ny = cfg["nx"], cfg["ny"]
+    nz = cfg["nz"] if cfg["dim"] == 3 else 1
+    n = nx * ny * nz
+    rng = np.random.default_rng(2)
+    u, v, w, p, t = ((rng.standard_normal(n) * 10.0 ** rng.integers(-6, 6, n)).astype(dt) for _ in range(5))
+    path = str(tmp_path / "out_bin.vtk")
+    ifc.write_vtk_host(cfg, u, v, w, p, t, path, binary=True)
+    r = read_legacy_binary_vtk(path)
+    assert r["header"] == ["# vtk DataFile Version 3.0", "flash 3d grid and solution", "BINARY",
+                           "DATASET RECTILINEAR_GRID", f"DIMENSIONS {nx + 1} {ny + 1} {nz + 1}"]
+    assert r["cell_data"] == f"CELL_DATA {n}" and r["field"] == "FIELD FieldData 3"
+    assert r["temperature_type"] == ("float" if prec == "f" else "double")
+    assert np.array_equal(r["temperature"], t)
+    assert np.array_equal(r["pressure"], p)
+    assert np.array_equal(r["velocity"], np.stack([u, v, w], axis=1).ravel())
+    for name, lo, hi, m in (("X_COORDINATES", "xmin", "xmax", nx), ("Y_COORDINATES", "ymin", "ymax", ny),
+                            ("Z_COORDINATES", "zmin", "zmax", nz)):
+        lo_t, d = dt(cfg[lo]), (dt(cfg[hi]) - dt(cfg[lo])) / dt(m)
+        assert np.array_equal(r[name], np.array([lo_t + dt(i) * d for i in range(m + 1)], dtype=dt)), name
+    # the ASCII file of the same fields: the same values to 6 significant digits
+    apath = str(tmp_path / "out.vtk")
+    ifc.write_vtk_host(cfg, u, v, w, p, t, apath)
+    lines = open(apath).read().split("\n")
+    ascii_p = np.array(lines[-1].split(), dtype=np.float64)
+    np.testing.assert_allclose(ascii_p, p.astype(np.float64), rtol=5e-6, atol=0)
