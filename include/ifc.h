@@ -329,9 +329,11 @@ int ifc_get_stats(ifc_solver *h, ifc_stats *stats);
  * FP64 sum of squared changes of each sweep.  stream: cudaStream_t or NULL.
  * Scratch comes from a fixed 152 KB array inside the library, held on every
  * GPU that loads it until the process exits.  Grids above 2^26 cells are
- * rejected with IFC_BAD_ARGUMENT and a message on stderr.  The first call on a
- * device looks the array's address up (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array, so calls that
+ * rejected with IFC_BAD_ARGUMENT and a message on stderr.  Every call looks
+ * the array's address up on the current device (cudaGetSymbolAddress), so a
+ * device reset between calls is safe; make the first call on a device before
+ * any stream capture, since it may load the module.  All calls share the
+ * array, so calls that
  * overlap on the GPU (from several streams or threads) race.  Returns when
  * the sweeps are done. */
 int ifc_rb_sweeps_noalloc(int dim, int nx, int ny, int nz, int precision, const void *coef, const void *src,

@@ -121,7 +121,7 @@ static __global__ void k_clear_stop(Ctl *ctl, int eq) { ctl->stop[eq] = 0; }
 template <typename T, int TX, int TY, int KS, int NT>
 __global__ void __launch_bounds__(NT) k_coef_solve2d(Params<T> P, const T *coef, const T *src, Ctl *ctl,
                                                      double *partials, GridBarrier *bar, int eq, int nsweeps, T *x0,
-                                                     T *x1)
+                                                     T *x1, int stall_test)
 {
     constexpr int H = 2 * KS;
     using R = Region<TX, TY, H>;
@@ -178,6 +178,10 @@ __global__ void __launch_bounds__(NT) k_coef_solve2d(Params<T> P, const T *coef,
     const T relax = g.relax[eq];
 
     for (int pass = 0; pass * KS < nsweeps && !stop; ++pass) {
+        // Failure-detection test (stall_test = 1): CTA 0 leaves without
+        // arriving, so every other CTA's bounded wait at this pass's barrier
+        // runs out and the launch ends with the timeout status.
+        if (stall_test && blockIdx.x == 0) { failed = true; break; }
         const int ns = clamp_sweeps(nsweeps, pass, KS);
         for (int q = tid; q < NR; q += NT) {
             const int a = q % W, b = q / W;

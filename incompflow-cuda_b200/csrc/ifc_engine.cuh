@@ -833,6 +833,10 @@ struct Engine : EngineBase {
         const long long N = g.N;
         T *src = f.tmp;
         IFC_CK(cudaStreamSynchronize(stream));
+        // A timeout of an earlier call leaves status 3 in the control block.
+        IFC_CK(cudaMemsetAsync(&ctl->status, 0, sizeof(int), stream));
+        const char *stall_env = std::getenv("IFC_TEST_STALL_BARRIER");
+        int stall_test = (stall_env && stall_env[0] == '1') ? 1 : 0;
         IFC_CK(cudaEventRecord(ev0, stream));
         if (dim == 2) k_temp_assemble<T, 2><<<grid(N), 256, 0, stream>>>(P, f, ta, f.mc, src);
         else k_temp_assemble<T, 3><<<grid(N), 256, 0, stream>>>(P, f, ta, f.mc, src);
@@ -885,7 +889,7 @@ struct Engine : EngineBase {
                 int ns_cycle = chunk, eq = EQ_W;
                 T *x1 = tbuf[1];
                 const T *coef = f.mc, *srcp = src_eff;
-                void *args[] = {&PT, &coef, &srcp, &ctl, &partials, &barrier, &eq, &ns_cycle, &f.temp, &x1};
+                void *args[] = {&PT, &coef, &srcp, &ctl, &partials, &barrier, &eq, &ns_cycle, &f.temp, &x1, &stall_test};
                 IFC_CK(cudaLaunchCooperativeKernel((const void *)k_coef_solve2d<T, S::TX, S::TY, kEnergyKS, S::NT>,
                                                    dim3(tiles), dim3(S::NT), args, R::NR * sizeof(T), stream));
                 ++launches;
@@ -910,6 +914,19 @@ struct Engine : EngineBase {
             IFC_CK(cudaGetLastError());
             int rc = read_ctl();
             if (rc != IFC_OK) return rc;
+            if (ctl_h.status == 3) {
+                // A grid barrier of the cooperative sweep launch gave up: the
+                // temperature may hold tiles of different passes.
+                err = "a grid barrier of the cooperative energy solve timed out";
+                if (res) {
+                    std::memset(res, 0, sizeof(*res));
+                    res->status = IFC_TIMEOUT;
+                }
+                k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << EQ_W);
+                IFC_CK(cudaMemsetAsync(&ctl->status, 0, sizeof(int), stream));
+                IFC_CK(cudaStreamSynchronize(stream));
+                return IFC_TIMEOUT;
+            }
             if (ctl_h.stop[EQ_W] && (!dc || ctl_h.sweeps[EQ_W] - cycle_start <= gran)) break;
         }
         IFC_CK(cudaEventRecord(ev1, stream));

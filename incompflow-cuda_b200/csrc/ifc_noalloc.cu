@@ -10,7 +10,6 @@
 // sweep kernel as ifc_sweep on buffers the caller owns, and takes its scratch
 // from a fixed array compiled into this library.
 #include <cstdio>
-#include <mutex>
 
 #include "ifc.h"
 #include "ifc_kernels.cuh"
@@ -33,21 +32,18 @@ constexpr size_t kScratchBytes = kCtlBytes + kPartialBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch on each device, looked up once per device.
-std::mutex g_mutex;
-void *g_scratch_ptr[64] = {};
-
+// Device address of g_noalloc_scratch on the current device.  It is looked up
+// on every call (a few microseconds next to two kernel launches and a stream
+// synchronisation) rather than cached: after cudaDeviceReset, or when the
+// primary context is torn down and recreated, the module is loaded again and
+// the array may sit at another address.
 int scratch_for_current_device(void **out)
 {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return IFC_CUDA_ERROR;
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return IFC_CUDA_ERROR;
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    if (cudaGetDevice(&dev) != cudaSuccess) return IFC_CUDA_ERROR;
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return IFC_CUDA_ERROR;
+    *out = p;
     return IFC_OK;
 }
 

@@ -23,7 +23,9 @@ struct velBCs {
     static constexpr int type[6] = {2, 1, 0, 0, 0, 0};
     static constexpr scalar val[6][3] = {{0, 0, 0}, {0.001, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 };
-// carried for the output surface; the energy equation is not solved
+// temperature BCs (0 given temperature, 1 zero gradient): used by the energy
+// solve on the converged flow (ifc_solve_energy); Solver::solve() itself solves
+// only the flow, as the reference does
 struct TempBCs {
     static constexpr int type[6] = {1, 1, 0, 0, 1, 1};
     static constexpr scalar val[6] = {0.0, 0.0, 293.0, 373.0, 0.0, 0.0};

@@ -26,6 +26,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 sys.path.insert(0, os.path.join(HERE, "..", "incompflow-cuda_b200", "python"))
 
+# Where the reference's sources lie on the machine that builds the checker;
+# IFC_REFERENCE_ROOT overrides it.
+DEFAULT_REF_ROOT = os.environ.get("IFC_REFERENCE_ROOT", "/root/reference")
+
 NVCC = ["nvcc", "-std=c++20", "-O2", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-O2"]
 
 
@@ -105,6 +109,17 @@ def cases():
     }
 
 
+def vtk_cases():
+    """Cases whose seeded fields the harness ref_vtk.cpp writes with the
+    reference's Solver::writeVTK: a 2D grid with non-unit extents and a small
+    3D box (the writer is host code; the Solver's constructor only allocates)."""
+    import ifc
+
+    mixed = kernel_cases()["mixed20x13"]
+    box = ifc.cavity3d(5, nx=5, ny=4, nz=3, xmin=-0.3, xmax=0.7, ymin=0.05, ymax=0.125, zmin=-1.5, zmax=2.25)
+    return {"vtk_mixed20x13": mixed, "vtk_box5x4x3": box}
+
+
 def build(ref_root: str, only=None):
     os.makedirs(OUT, exist_ok=True)
     inc = os.path.join(ref_root, "include")
@@ -133,12 +148,22 @@ def build(ref_root: str, only=None):
         kexe = os.path.join(OUT, f"ref_kernels_{name}")
         subprocess.run(NVCC + [f"-I{d}", f"-I{inc}", os.path.join(HERE, "ref_kernels.cu"), "-o", kexe], check=True)
         built.append(kexe)
+    for name, c in vtk_cases().items():
+        if only and name not in only:
+            continue
+        d = os.path.join(OUT, f"cfg_{name}")
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "config.h"), "w") as fh:
+            fh.write(config_h(c, 1, 0.0, 0.0, 0.0))
+        vexe = os.path.join(OUT, f"ref_{name}")
+        subprocess.run(NVCC + [f"-I{d}", f"-I{inc}", src, os.path.join(HERE, "ref_vtk.cpp"), "-o", vexe], check=True)
+        built.append(vexe)
     return built
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=DEFAULT_REF_ROOT)
     ap.add_argument("--only", nargs="*")
     a = ap.parse_args()
     for b in build(a.ref_root, a.only):

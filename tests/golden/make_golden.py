@@ -9,6 +9,10 @@ machine after `python oracle/build_ref.py` has compiled oracle/_ref/).
 * ref_solve_<case>.npz: u, v, p of the reference's Solver::solve() after a
   fixed number of outer iterations well past convergence, read back from its
   VTK output (6 significant digits).
+* ref_vtk_<case>.npz (--vtk-only; runs on a machine without a GPU, since the
+  writer is host code and the Solver's constructor only allocates): seeded
+  float32 fields and the bytes the reference's Solver::writeVTK wrote from
+  them (oracle/ref_vtk.cpp).
 * oracle_cavity3d16.npz (--oracle-only needs no GPU): the 16^3 lid-driven
   cavity solved by the FP64 oracle (red-black Gauss-Seidel, per-field rule
   1e-5).  The reference's 3D build cannot run (it launches 2048-thread blocks
@@ -72,6 +76,39 @@ def run_solve_case(name: str, n_cells: int, out: str):
     np.savez_compressed(os.path.join(out, f"ref_solve_{name}.npz"), u=u, v=v, p=p, log=np.array(r.stdout[-2000:]))
 
 
+def vtk_fields(cfg: dict, seed: int) -> dict:
+    """Seeded float32 fields spanning many magnitudes (mantissas times 10^-9 ..
+    10^9, zeros, small integers, negative values), so the reference's %g-like
+    output meets fixed and exponent forms, trailing-zero removal and rounding."""
+    rng = np.random.default_rng(seed)
+    nz = cfg.get("nz", 1) if cfg["dim"] == 3 else 1
+    n = cfg["nx"] * cfg["ny"] * nz
+    out = {}
+    for k in ("u", "v", "w", "p", "T"):
+        x = rng.uniform(-10, 10, n) * 10.0 ** rng.integers(-9, 10, n)
+        pick = rng.random(n)
+        x[pick < 0.05] = 0.0
+        sel = (pick >= 0.05) & (pick < 0.12)
+        x[sel] = rng.integers(-1000, 1000, int(sel.sum()))
+        out[k] = x.astype(np.float32)
+    return out
+
+
+def run_vtk_case(name: str, cfg: dict, out: str):
+    """The reference's Solver::writeVTK on seeded fields (ref_vtk.cpp): the
+    file's bytes and the fields they were written from."""
+    f = vtk_fields(cfg, seed=7)
+    with tempfile.TemporaryDirectory() as tmp:
+        din = os.path.join(tmp, "in")
+        os.makedirs(din)
+        for k, v in f.items():
+            v.tofile(os.path.join(din, f"{k}.bin"))
+        subprocess.run([os.path.join(REF, f"ref_{name}"), din, f"{name}.vtk"], cwd=tmp, check=True,
+                       capture_output=True)
+        data = open(os.path.join(tmp, "output", f"{name}.vtk"), "rb").read()
+    np.savez_compressed(os.path.join(out, f"ref_{name}.npz"), **f, vtk=np.frombuffer(data, dtype=np.uint8))
+
+
 def oracle_cavity3d(out: str):
     import ifc
     import oracle as O
@@ -93,8 +130,13 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--oracle-only", action="store_true")
+    ap.add_argument("--vtk-only", action="store_true", help="only the writeVTK fixtures (host code; no GPU needed)")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
+    for name, cfg in build_ref.vtk_cases().items():
+        run_vtk_case(name, cfg, a.out)
+    if a.vtk_only:
+        return
     oracle_cavity3d(a.out)
     if a.oracle_only:
         return

@@ -10,6 +10,7 @@ the CPU oracle under the reference's own stopping rule.
 import os
 import shutil
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -20,7 +21,10 @@ from helpers import rel_l2, to_oracle_cfg
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "incompflow-cuda_b200")
-REF_MAIN = "/root/reference/main.cpp"
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from build_ref import DEFAULT_REF_ROOT  # noqa: E402
+
+REF_MAIN = os.path.join(DEFAULT_REF_ROOT, "main.cpp")
 
 
 def write_case(d, cfg, scalar="float"):

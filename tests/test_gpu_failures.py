@@ -42,3 +42,23 @@ def test_grid_barrier_timeout_is_reported_and_device_stays_usable(gpu_ok, monkey
     st = t.iterate(3)
     assert st["status"] == ifc.OK and st["outer_iterations"] == 3
     assert np.isfinite(t.get("u")).all()
+
+
+def test_energy_barrier_timeout_is_reported_and_handle_stays_usable(gpu_ok, monkeypatch):
+    """The cooperative 2D energy launch (k_coef_solve2d) with CTA 0 leaving
+    before its first grid barrier: the other CTAs' bounded waits run out,
+    solve_energy returns TIMEOUT, and the same handle then solves normally."""
+    monkeypatch.delenv("IFC_PERSIST_OFF", raising=False)
+    cfg = ifc.cavity2d(32)
+    s = ifc.Solver(cfg)
+    s.iterate(50)
+    monkeypatch.setenv("IFC_TEST_STALL_BARRIER", "1")
+    with pytest.raises(ifc.IfcError) as e:
+        s.solve_energy(max_sweeps=40, tol=0.0)
+    assert e.value.status == ifc.TIMEOUT
+    monkeypatch.delenv("IFC_TEST_STALL_BARRIER")
+    r = s.solve_energy(max_sweeps=40, tol=0.0)
+    assert r["status"] == ifc.OK and r["sweeps"] == 40
+    assert np.isfinite(s.get("T")).all()
+    st = s.iterate(3)
+    assert st["status"] == ifc.OK

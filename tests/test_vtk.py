@@ -30,6 +30,25 @@ def expected_vtk(cfg, u, v, w, p, t, dtype):
     return "".join(s)
 
 
+@pytest.mark.parametrize("case", ["vtk_mixed20x13", "vtk_box5x4x3"])
+def test_vtk_bytes_equal_the_reference_writers(tmp_path, case):
+    """Files written by the reference's own Solver::writeVTK (src/Solver.cu:
+    301-367) from seeded FP32 fields (tests/golden/ref_<case>.npz, made by
+    tests/golden/make_golden.py --vtk-only through oracle/ref_vtk.cpp): the
+    library's writer, given the same fields, reproduces every byte."""
+    import os
+
+    import build_ref
+
+    cfg = build_ref.vtk_cases()[case]
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"ref_{case}.npz"))
+    path = str(tmp_path / "out.vtk")
+    ifc.write_vtk_host(cfg, g["u"], g["v"], g["w"], g["p"], g["T"], path)
+    mine, ref = open(path, "rb").read(), g["vtk"].tobytes()
+    assert len(mine) == len(ref)
+    assert mine == ref
+
+
 @pytest.mark.parametrize("prec", ["f", "d"])
 @pytest.mark.parametrize("cfg", [ifc.channel2d(12, 5), ifc.cavity3d(4, nx=4, ny=3, nz=5)])
 def test_vtk_bytes(tmp_path, cfg, prec):

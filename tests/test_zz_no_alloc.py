@@ -66,3 +66,36 @@ def test_noalloc_rejects_oversize_grid(gpu_ok, capfd):
     rc = noalloc()(3, 1024, 1024, 1024, 0, None, None, None, 0.7, 1, None, None)
     assert rc == ifc.BAD_ARGUMENT
     assert "exceed the maximum" in capfd.readouterr().err
+
+
+def test_noalloc_grid_stride_path_on_caller_stream(gpu_ok):
+    """A 1024 x 600 FP32 grid: 307,200 cells of each colour need more than the
+    1024 blocks of 256 threads the entry point launches, so its kernel walks
+    the grid in strides.  The call goes on a caller-created stream, twice in
+    a row, and must equal the handle's sweeps bit for bit."""
+    import torch
+
+    cfg = ifc.cavity2d(1024, ny=600)
+    s = ifc.Solver(cfg)
+    for k, v in seeded_state(cfg, 5, s.dtype).items():
+        s.set(k, v)
+    s.stage("face_bc")
+    s.stage("mom_assemble")
+    d_coef = torch.from_numpy(s.get("mcoef")).cuda()
+    d_src = torch.from_numpy(s.get("src_u")).cuda()
+    d_phi = torch.from_numpy(s.get("u")).cuda()
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    fn = noalloc()
+    for call, n in enumerate((2, 1)):
+        ref_sq = s.sweep(0, n)
+        ref_u = s.get("u")
+        sq = (C.c_double * n)()
+        rc = fn(2, s.nx, s.ny, 1, 0, d_coef.data_ptr(), d_src.data_ptr(), d_phi.data_ptr(), cfg["relax_u"], n, sq,
+                stream.cuda_stream)
+        assert rc == ifc.OK, (call, rc)
+        stream.synchronize()
+        got = d_phi.cpu().numpy()
+        assert np.array_equal(got, ref_u), (call, int((got != ref_u).sum()))
+        np.testing.assert_allclose(np.array(sq[:n]), ref_sq, rtol=1e-12)
+    s.close()
