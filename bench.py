@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the compact precision / batch / adjoint records of the default line")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--form", default="plain",
                     choices=["plain", "adjoint", "precision", "batch", "convergence", "energy"],
@@ -82,6 +84,14 @@ def workload_cfg():
 
 def workload_name():
     return WORKLOAD if CONVECTION == "upwind" else f"{WORKLOAD}_{CONVECTION}"
+
+
+def workload_config() -> dict:
+    """The workload as both arms report it (the same dict in each line)."""
+    cfg = workload_cfg()
+    return {"workload": workload_name(), "nx": 512, "ny": 128, "outer_iterations_per_step": OUTER_PER_STEP,
+            "convection": CONVECTION, "sweeps_u_v_p": [cfg["nIter_u"], cfg["nIter_v"], cfg["nIter_p"]],
+            "relax_u_p": [cfg["relax_u"], cfg["relax_p"]], "start": "from rest", "scalar": "fp32"}
 
 
 def measured_peaks():
@@ -305,12 +315,10 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic: flow from rest, advanced by the warm-up steps",
-            "config": {"workload": workload_name(), "nx": 512, "ny": 128,
-                       "outer_iterations_per_step": OUTER_PER_STEP, "convection": CONVECTION,
-                       "sweeps_u_v_p": [cfg["nIter_u"], cfg["nIter_v"], cfg["nIter_p"]],
-                       "linear_solver": "red-black Gauss-Seidel", "precision": "fp32 sweeps, fp64 norms",
-                       "l2": "flushed (256 MB write) between timed steps",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(),
+            "impl_notes": {"linear_solver": "red-black Gauss-Seidel", "precision": "fp32 sweeps, fp64 norms",
+                           "l2": "flushed (256 MB write) between timed steps",
+                           "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_upd_all / (e2e_all * 1e-3), "unit": METRIC,
                     "h2d_bytes_per_step": 3 * nbytes, "d2h_bytes_per_step": 3 * nbytes},
             "gpu_launches": launches,
@@ -325,11 +333,177 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_forms and CONVECTION == "upwind":
+            forms = {}
+            for name, fn in (("precision", lambda: precision_summary(args.n3d)),
+                             ("batch", lambda: batch_summary(4)), ("adjoint", lambda: adjoint_summary(4, 8))):
+                t0 = time.perf_counter()
+                try:
+                    forms[name] = fn()
+                except Exception as e:  # a form's failure must not cost the headline line
+                    forms[name] = {"error": f"{type(e).__name__}: {e}"}
+                forms[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+            line["forms"] = forms
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---- compact records of the three further forms in the default line --------
+# Each runs after the headline's timed region, on rank 0 at N = 1, and takes
+# seconds; the full forms are bench.py --form precision|batch|adjoint.
+
+def rel_l2(a, b):
+    import numpy as np
+
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def prec_byte_model(cfg: dict, N: int) -> dict:
+    """Compulsory unique bytes of each 3D stage launch sequence (FP32, whole
+    arrays per pass: a half sweep reads whole cache lines of both colours)."""
+    nu, npc = cfg["nIter_u"], cfg["nIter_p"]
+    return {
+        "mom_solve": (nu * 2 * (3 * 4 + 4 + 6 * 4)) * N,          # per half: faces, p, u/v/w read+write
+        "rhie_chow": (3 * 4 + 4 + 4 + 3 * 4 + 3 * 4 + 4) * N,     # u v w, p, aC in; faces, b_p out
+        "pcorr_solve": (4 + 4 + npc * 2 * (4 + 4 + 4 + 4)) * N,   # 1/aC once; per half 1/aC, p', b_p, p' write
+        "update": (4 + 4 + 4 * 3 + 3 * 4 + 4 + 3 * 4 * 2 + 4) * N,
+    }
+
+
+def precision_summary(n: int) -> dict:
+    """The 128^3 cavity at Re 400: FP32 time to convergence, ms per outer
+    iteration, each stage's compulsory bytes over its device time against the
+    measured HBM peak, and the FP32 fields against the FP64 build after the
+    same number of outer iterations."""
+    import numpy as np
+
+    import ifc
+
+    cfg = ifc.cavity3d(n, re=400.0, numOuterIter=8000)
+    crit = ifc.CRIT_REFERENCE
+    s32 = ifc.Solver(dict(cfg, precision="f", criterion=crit))
+    st = s32.solve()
+    k = st["outer_iterations"]
+    peak, _ = measured_peaks()
+    model = prec_byte_model(cfg, n ** 3)
+    stages = {}
+    for name in ("mom_solve", "rhie_chow", "pcorr_solve", "update"):
+        ms_, nl = s32.time_stage(name, reps=3)
+        gbs = model[name] / (ms_ * 1e-3) / 1e9
+        stages[name] = {"ms": round(ms_, 4), "launches": nl, "gbs": round(gbs, 1), "frac_of_peak": round(gbs / peak, 3)}
+    a = {f: s32.get(f).astype(np.float64) for f in ("u", "v", "w", "p")}
+    s32.close()
+    s64 = ifc.Solver(dict(cfg, precision="d"))
+    st64 = s64.iterate(k)
+    b = {f: s64.get(f) for f in ("u", "v", "w", "p")}
+    s64.close()
+    a["p"] -= a["p"].mean()
+    b["p"] = b["p"] - b["p"].mean()
+    return {"workload": f"cavity3d_{n}_re400", "criterion": "reference rule (norms over the p-norm max), 1e-5",
+            "fp32_converged": bool(st["converged"]), "outer_iterations": k,
+            "seconds_to_convergence": st["device_ms"] / 1e3, "ms_per_outer_iteration": st["device_ms"] / max(k, 1),
+            "fp64_ms_per_outer_iteration": st64["device_ms"] / max(k, 1),
+            "rel_l2_vs_fp64_build_equal_iterations": {f: rel_l2(a[f], b[f]) for f in a},
+            "stages_at_convergence": stages, "hbm_peak_gbs": peak,
+            "gpu_launches": st["kernel_launches"] + st64["kernel_launches"]}
+
+
+def batch_summary(every: int) -> dict:
+    """Every `every`-th case of the seeded 256-case cavity batch: one batched
+    solve against the plain per-case loop (sum of per-case device times)."""
+    import numpy as np
+
+    import ifc
+
+    sub = ifc.batch_cases(256, seed=0)[::every]
+    ifc.batch_solve([ifc.cavity2d(32), ifc.cavity2d(128), ifc.cavity2d(256)], want_fields=False)  # autotune
+    res, fields, bms = ifc.batch_solve(sub)
+    plain_ms, worst, conv_p = 0.0, 0.0, 0
+    for q, c in enumerate(sub):
+        s = ifc.Solver(c)
+        st = s.solve()
+        plain_ms += st["device_ms"]
+        conv_p += int(st["converged"])
+        for f in ("u", "v"):
+            worst = max(worst, rel_l2(fields[q][f], s.get(f)))
+        s.close()
+    return {"workload": f"batch_cavity2d_256_every{every}", "cases": len(sub),
+            "solves_per_s": len(sub) / (bms * 1e-3), "plain_loop_solves_per_s": len(sub) / (plain_ms * 1e-3),
+            "speedup_vs_plain": plain_ms / bms, "batch_ms": bms, "plain_loop_ms": plain_ms,
+            "converged": {"batch": int(sum(r["converged"] for r in res)), "plain": conv_p, "of": len(sub)},
+            "max_rel_l2_batch_vs_plain_uv": worst, "criterion": "per-field relative 1e-5"}
+
+
+def adjoint_summary(nprof: int, fd_every: int) -> dict:
+    """nprof seeded inlet profiles of the 256 x 64 channel: FP32 primal solve
+    and FP64 adjoint device times; the first profile's gradient against FP64
+    central differences for every fd_every-th inlet parameter and mu."""
+    import numpy as np
+
+    import ifc
+
+    nx, ny = 256, 64
+    base = ifc.channel2d(nx, ny, inlet_profile=adjoint_profile(0))
+    s32 = ifc.Solver(base)
+    s32.solve()
+    s32.adjoint(tol=1e-8)  # warm-up
+    rows = []
+    for k in range(nprof):
+        s32.set_inlet_profile(adjoint_profile(k, ny))
+        s32.set_uniform()
+        st = s32.solve()
+        dth, res = s32.adjoint(tol=1e-8)
+        rows.append((st["device_ms"], res["device_ms"], dth, res["dJ_dmu"], st["converged"] and res["converged"]))
+    s32.close()
+    theta = adjoint_profile(0, ny)
+    c64 = dict(base, precision="d", inlet_profile=theta)
+    s64 = ifc.Solver(c64)
+    s64.solve()
+    s64.iterate(4000)
+    keys = ("u", "v", "p", "uf", "vf")
+    state = {f: s64.get(f) for f in keys}
+
+    def J_from(sol):
+        for f, a_ in state.items():
+            sol.set(f, a_)
+        sol.iterate(3000)
+        p_ = sol.get("p").reshape(ny, nx)
+        return float(p_[:, 0].mean() - p_[:, -1].mean())
+
+    errs = []
+    for j in range(0, ny, fd_every):
+        h = 1e-3 * theta[j]
+        Js = []
+        for sgn in (1.0, -1.0):
+            tt = theta.copy()
+            tt[j] += sgn * h
+            s64.set_inlet_profile(tt)
+            Js.append(J_from(s64))
+        fd = (Js[0] - Js[1]) / (2 * h)
+        errs.append(abs(rows[0][2][j] - fd) / abs(fd))
+    s64.close()
+    mu = base["dynamicViscosity"]
+    Jm = []
+    for sgn in (1.0, -1.0):
+        sm = ifc.Solver(dict(c64, dynamicViscosity=mu + sgn * 1e-3 * mu))
+        Jm.append(J_from(sm))
+        sm.close()
+    fdmu = (Jm[0] - Jm[1]) / (2e-3 * mu)
+    errs.append(abs(rows[0][3] - fdmu) / abs(fdmu))
+    ratio = np.array([r[1] / r[0] for r in rows])
+    return {"workload": "channel2d_256x64_adjoint", "profiles": nprof,
+            "adjoint_over_primal": float(ratio.mean()), "ratio_max": float(ratio.max()), "bound": 3.0,
+            "primal_ms_mean": float(np.mean([r[0] for r in rows])),
+            "adjoint_ms_mean": float(np.mean([r[1] for r in rows])),
+            "all_converged": bool(all(r[4] for r in rows)),
+            "fd_check": {"profile": 0, "parameters": len(errs), "which": f"theta[::{fd_every}] and mu",
+                         "fd": "FP64 central, relative step 1e-3", "max_rel_err": float(max(errs)),
+                         "bound": 1e-4}}
 
 
 ADJ_WORKLOAD = "channel2d_256x64_adjoint"
@@ -533,15 +707,7 @@ def run_precision(args):
     err = {k: {"rel_l2": float(np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k])),
                "linf_rel": float(np.abs(a[k] - b[k]).max() / np.abs(b[k]).max())} for k in a}
     N = n ** 3
-    nu, npc = cfg["nIter_u"], cfg["nIter_p"]
-    # compulsory unique bytes per launch sequence, FP32 (whole arrays; a half
-    # sweep reads whole cache lines of both colours)
-    byte_model = {
-        "mom_solve": (nu * 2 * (3 * 4 + 4 + 6 * 4)) * N,          # per half: faces, p, u/v/w read+write
-        "rhie_chow": (3 * 4 + 4 + 4 + 3 * 4 + 3 * 4 + 4) * N,     # u v w, p, aC in; faces, b_p out
-        "pcorr_solve": (4 + 4 + npc * 2 * (4 + 4 + 4 + 4)) * N,   # 1/aC once; per half 1/aC, p', b_p, p' write
-        "update": (4 + 4 + 4 * 3 + 3 * 4 + 4 + 3 * 4 * 2 + 4) * N,
-    }
+    byte_model = prec_byte_model(cfg, N)
     peak, peak_kind = measured_peaks()
     stages = {}
     for name in ("mom_solve", "rhie_chow", "pcorr_solve", "update"):
@@ -584,8 +750,13 @@ def run_batch(args):
 
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     cases = ifc.batch_cases(args.cases, seed=0)
-    mine = ifc.shard_cases([c["nx"] * c["ny"] for c in cases], rank, world) if world > 1 else list(range(len(cases)))
+    mine = ifc.shard_cases([ifc.case_weight(c) for c in cases], rank, world) if world > 1 else list(range(len(cases)))
     sub = [cases[i] for i in mine]
     # warm-up: one case of every size class, which also runs the autotuner
     # (it times each variant once per class and process); its time is reported
@@ -615,26 +786,57 @@ def run_batch(args):
             b = s.get(f).astype(np.float64)
             worst = max(worst, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
         s.close()
+    local_res = {"solves": len(sub), "updates": updates, "case_its": case_its, "conv_batch": nconv_b,
+                 "conv_plain": nconv_p, "batch_ms": bms, "plain_ms": plain_ms, "worst": worst}
+    tot = batch_totals(local_res, world, torch.device("cuda", local))
     line = {
-        "metric": "converged solves/s", "value": len(sub) / (bms * 1e-3), "unit": "solves/s",
-        "higher_is_better": True, "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": bms,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded cavity cases from rest",
-        "config": {"workload": f"batch_cavity2d_{args.cases}", "cases_this_rank": len(sub),
+        "metric": "converged solves/s", "value": tot["solves"] / (tot["batch_ms"] * 1e-3), "unit": "solves/s",
+        "higher_is_better": True, "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": tot["batch_ms"],
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded cavity cases from rest",
+        "config": {"workload": f"batch_cavity2d_{args.cases}", "cases": int(tot["solves"]),
                    "sizes": "nx, ny in {32..256 step 32}", "re": "log-uniform [10, 1000]",
-                   "criterion": "per-field relative 1e-5"},
-        "plain_loop": {"solves_per_s": len(sub) / (plain_ms * 1e-3), "device_ms": plain_ms,
-                       "note": "sum of per-case ifc_solve device times, handle creation excluded"},
-        "speedup_vs_plain": plain_ms / bms,
-        "case_outer_iterations": case_its,
-        "cell_updates_per_s": updates / (bms * 1e-3),
-        "variants_used": variants,
+                   "criterion": "per-field relative 1e-5",
+                   "sharding": "greedy longest-first by ifc.case_weight, no data-path collective"},
+        "plain_loop": {"solves_per_s": tot["solves"] / (tot["plain_ms"] * 1e-3), "device_ms": tot["plain_ms"],
+                       "note": "per rank the sum of per-case ifc_solve device times (handle creation excluded), "
+                               "max over ranks"},
+        "speedup_vs_plain": tot["plain_ms"] / tot["batch_ms"],
+        "case_outer_iterations": int(tot["case_its"]),
+        "cell_updates_per_s": tot["updates"] / (tot["batch_ms"] * 1e-3),
+        "variants_used_rank0": variants,
         "autotune_and_warmup_seconds": tune_s,
-        "converged": {"batch": nconv_b, "plain": nconv_p, "of": len(sub)},
-        "max_rel_l2_batch_vs_plain_uv": worst,
+        "converged": {"batch": int(tot["conv_batch"]), "plain": int(tot["conv_plain"]), "of": int(tot["solves"])},
+        "max_rel_l2_batch_vs_plain_uv": tot["worst"],
         "clocks": clk,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def batch_totals(local: dict, world: int, device) -> dict:
+    """Whole-job totals of the batch form over the ranks of the process group:
+    solves, cell-updates, case iterations and converged counts are summed;
+    device times (each rank's batch and plain-loop time) and the worst field
+    difference take the maximum.  world == 1 returns the local values."""
+    if world == 1:
+        return dict(local)
+    import torch
+    import torch.distributed as dist
+
+    sums = ("solves", "updates", "case_its", "conv_batch", "conv_plain")
+    maxes = ("batch_ms", "plain_ms", "worst")
+    a = torch.tensor([float(local[k]) for k in sums], dtype=torch.float64, device=device)
+    b = torch.tensor([float(local[k]) for k in maxes], dtype=torch.float64, device=device)
+    dist.all_reduce(a, op=dist.ReduceOp.SUM)
+    dist.all_reduce(b, op=dist.ReduceOp.MAX)
+    out = dict(zip(sums, a.tolist()))
+    out.update(zip(maxes, b.tolist()))
+    return out
 
 
 ENERGY_SWEEPS = 2000
@@ -832,7 +1034,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: flow from rest",
-        "config": {"workload": WORKLOAD, "nx": 512, "ny": 128, "outer_iterations_per_step": OUTER_PER_STEP},
+        "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)

@@ -461,6 +461,13 @@ def batch_cases(n: int = 256, seed: int = 0, sizes=(32, 64, 96, 128, 160, 192, 2
     return out
 
 
+def case_weight(cfg: dict) -> float:
+    """Weight of one batch case for sharding: its cells times cells^0.4, since
+    larger cases also take more outer iterations to converge."""
+    n = cfg["nx"] * cfg["ny"] * (cfg.get("nz", 1) if cfg["dim"] == 3 else 1)
+    return n * n ** 0.4
+
+
 def shard_cases(weights: list, rank: int, world: int) -> list:
     """Indices of the cases rank `rank` of `world` solves: a greedy
     longest-first split of the case weights (cells x expected iterations) over

@@ -103,6 +103,9 @@ def cases():
         # convergence (the reference's own stopping rule is defective, D6/D7)
         "cavity64": (ifc.cavity2d(64), 3000, 0.0, 0.0, 0.0),
         "channel128x32": (ifc.channel2d(128, 32), 3000, 0.0, 0.0, 0.0),
+        # the bench case itself, 10000 outer iterations from rest in one
+        # solve() call (the oracle converges it in about 6300)
+        "channel512x128_long": (ifc.channel2d(512, 128), 10000, 0.0, 0.0, 0.0),
         # time to convergence by the reference's own stopping rule (configs[0]:
         # the 64^2 cavity at tolerance 1e-5, no mass-norm stop)
         "cavity64_converge": (ifc.cavity2d(64), 20000, 1e-5, 1e-5, 0.0),

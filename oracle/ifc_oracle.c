@@ -24,4 +24,7 @@
 /* Reverse pass of one outer iteration (FP64, 2D), see ifc_adjoint_impl.h. */
 #include "ifc_adjoint_impl.h"
 
+/* Continue a solve from loaded fields: outer iteration `it` > 0 skips the
+ * face initialisation of the first iteration (include/kernels.cuh:10-45). */
+void orc_set_iteration_count_f(orc_state_f *s, int it) { s->it = it; }
 void orc_set_iteration_count_d(orc_state_d *s, int it) { s->it = it; }

@@ -118,6 +118,7 @@ ORC_DECLARE(double, d)
 int orc_adjoint_apply_d(orc_state_d *s, const double *lu_in, const double *lv_in, const double *lp_in,
                         const double *luf_in, const double *lvf_in, double *lu_out, double *lv_out, double *lp_out,
                         double *luf_out, double *lvf_out, double *ltheta, double *lmu);
+void orc_set_iteration_count_f(orc_state_f *s, int it);
 void orc_set_iteration_count_d(orc_state_d *s, int it);
 
 #ifdef __cplusplus

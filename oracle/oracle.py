@@ -96,8 +96,10 @@ def lib():
         PD = C.POINTER(C.c_double)
         _lib.orc_adjoint_apply_d.restype = C.c_int
         _lib.orc_adjoint_apply_d.argtypes = [C.c_void_p] + [PD] * 12
-        _lib.orc_set_iteration_count_d.restype = None
-        _lib.orc_set_iteration_count_d.argtypes = [C.c_void_p, C.c_int]
+        for s in ("f", "d"):
+            fn = getattr(_lib, f"orc_set_iteration_count_{s}")
+            fn.restype = None
+            fn.argtypes = [C.c_void_p, C.c_int]
     return _lib
 
 
@@ -211,6 +213,11 @@ class Oracle:
     def iterations(self) -> int:
         return self._fn("iteration_count")(self._h)
 
+    def set_iteration_count(self, it: int):
+        """Continue from loaded fields: a count > 0 skips the face
+        initialisation of the first outer iteration."""
+        self._fn("set_iteration_count")(self._h, it)
+
 
 def _ptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
@@ -240,9 +247,6 @@ class AdjointOracle(Oracle):
                                        C.byref(lmu))
         assert rc == 0
         return outs, lth, lmu.value
-
-    def set_iteration_count(self, it: int):
-        lib().orc_set_iteration_count_d(self._h, it)
 
     def objective_seed(self):
         """dJ/dx of J = mean p over the first cell column - mean over the last."""

@@ -104,12 +104,17 @@ def test_iterate_fixed_count_and_continue(gpu_ok):
     assert rel_l2(s.get("u"), o.field("u")) < 1e-6
 
 
-@pytest.mark.parametrize("name,closed", [("cavity64", True), ("channel128x32", False)])
-def test_device_matches_reference_build(gpu_ok, name, closed):
+@pytest.mark.parametrize("name,closed,bound", [("cavity64", True, 1e-5), ("channel128x32", False, 1e-5),
+                                               ("channel512x128_long", False, 3e-5)])
+def test_device_matches_reference_build(gpu_ok, name, closed, bound):
     """The device solver against the reference's own CUDA build (fixtures in
-    tests/golden/, produced by its Solver::solve() on a B200): the same 3000
-    outer iterations from rest; bound 1e-5 relative L2, the resolution of the
-    reference's 6-digit VTK output being ~1e-6 (the north star asks 1e-4)."""
+    tests/golden/, produced by its Solver::solve() on a B200): the same outer
+    iterations from rest (3000; 10000 for the 512 x 128 bench channel, in one
+    solve() call); bound 1e-5 relative L2, the resolution of the
+    reference's 6-digit VTK output being ~1e-6 (the north star asks 1e-4).
+    On the 512 x 128 channel both FP32 solutions sit at the FP32 round-off
+    floor of the pressure, 1.2e-5 apart (each 5e-5 from the FP64 answer), so
+    that case is held to 3e-5."""
     import os
 
     import build_ref
@@ -121,11 +126,11 @@ def test_device_matches_reference_build(gpu_ok, name, closed):
     st = s.iterate(n_outer)
     assert st["outer_iterations"] == n_outer
     for k in ("u", "v"):
-        assert rel_l2(s.get(k), g[k]) < 1e-5, (k, rel_l2(s.get(k), g[k]))
+        assert rel_l2(s.get(k), g[k]) < bound, (k, rel_l2(s.get(k), g[k]))
     p, pr = s.get("p").astype(np.float64), g["p"]
     if closed:
         p, pr = p - p.mean(), pr - pr.mean()
-    assert rel_l2(p, pr) < 1e-5, rel_l2(p, pr)
+    assert rel_l2(p, pr) < bound, rel_l2(p, pr)
 
 
 @pytest.mark.parametrize("sweeps_per_pass", [5, 4, 3])
