@@ -47,8 +47,14 @@ enum { IFC_FP32 = 0, IFC_FP64 = 1 };
 enum { IFC_GAUSS_SEIDEL = 0, IFC_JACOBI = 1 };
 /* Convergence rule.  REFERENCE reproduces src/Solver.cu:237-268 exactly,
  * including the division of every norm by the running max of the pressure norm;
- * PER_FIELD divides each norm by its own running max (FP64). */
-enum { IFC_CRIT_REFERENCE = 0, IFC_CRIT_PER_FIELD = 1 };
+ * PER_FIELD divides each norm by its own running max (FP64).  RESIDUAL (an
+ * addition; not in the batched form) applies the per-field rule to FP64
+ * residuals instead of corrections: u, v, w by the RMS of their assembled
+ * momentum equation's residual b - aC phi - sum a_nb phi_nb at the start of
+ * the outer iteration (tolerances tol_u, tol_v, tol_w), p by the RMS mass
+ * imbalance (tol_p); in FP32 the correction norms level off at the rounding
+ * noise of the corrected fields, these residuals do not. */
+enum { IFC_CRIT_REFERENCE = 0, IFC_CRIT_PER_FIELD = 1, IFC_CRIT_RESIDUAL = 2 };
 
 /* Convection schemes of the momentum equations.  IFC_CONV_UPWIND is the
  * reference's first-order upwind (include/kernels.cuh:97-134) and the default;
@@ -102,7 +108,7 @@ typedef struct ifc_config {
     /* ---- additions ---- */
     int precision;                    /* IFC_FP32 (default) or IFC_FP64 */
     int linear_solver;                /* IFC_GAUSS_SEIDEL (default) or IFC_JACOBI */
-    int criterion;                    /* IFC_CRIT_PER_FIELD (default) or IFC_CRIT_REFERENCE */
+    int criterion;                    /* IFC_CRIT_PER_FIELD (default), _REFERENCE or _RESIDUAL */
     int pin_pressure;                 /* -1 auto (closed domains), 0 off, 1 on */
     int sweeps_per_pass;              /* sweeps fused per device pass; 0 = tuned default */
     int log_level;                    /* 0 silent, 1 reference log cadence on stdout */
@@ -342,6 +348,12 @@ int ifc_rb_sweeps_noalloc(int dim, int nx, int ny, int nz, int precision, const 
 const char *ifc_status_string(int status);
 const char *ifc_last_error(const ifc_solver *h);
 int ifc_abi_version(void);
+/* Build options of the loaded library (an addition; the reference has one
+ * build): IFC_BUILD_BOUNDS_CHECK when it was compiled with IFC_BOUNDS_CHECK,
+ * whose kernels check every field-array index and report an out-of-range
+ * one as IFC_BAD_ARGUMENT instead of touching the memory. */
+enum { IFC_BUILD_BOUNDS_CHECK = 1 };
+int ifc_build_flags(void);
 
 #ifdef __cplusplus
 }

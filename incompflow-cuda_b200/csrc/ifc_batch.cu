@@ -833,7 +833,8 @@ extern "C" int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result 
     for (int c = 0; c < n; ++c) {
         const int rc = ifc_config_check(&cases[c]);
         if (rc != IFC_OK) return rc;
-        if (cases[c].dim != 2 || cases[c].linear_solver != IFC_GAUSS_SEIDEL || cases[c].precision != prec)
+        if (cases[c].dim != 2 || cases[c].linear_solver != IFC_GAUSS_SEIDEL || cases[c].precision != prec ||
+            cases[c].criterion == IFC_CRIT_RESIDUAL)
             return IFC_UNSUPPORTED;
     }
     try {

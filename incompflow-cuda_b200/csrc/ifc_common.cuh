@@ -35,20 +35,57 @@ struct Geo {
     int closed[6];                  // face pressure = cell pressure (wall or inlet)
     T bcv[6][3];
     const T *inlet;                 // west-face inlet profile (device, ny*nz) or nullptr
-    int criterion;                  // 0 reference rule, 1 per-field rule
+    int criterion;                  // 0 reference rule, 1 per-field rule, 2 per field on FP64 residuals
     int conv;                       // convection scheme (ifc_convection.cuh); 0 upwind
 };
 
+#ifdef IFC_BOUNDS_CHECK
+// Bounds-checked build (make lib_bc): every field array is a view that knows
+// its length.  An index outside [0, n) records the index in a device flag and
+// is redirected to a scratch slot -- no trap, the context stays usable -- and
+// the host returns IFC_BAD_ARGUMENT after the launch sequence.  Pointer
+// copies taken from a view (T *x = f.u) are not checked.
+static __device__ int g_ifc_bounds_err;
+static __device__ unsigned long long g_ifc_bounds_idx;
+static __device__ double g_ifc_bounds_sink[64];
+
+template <typename T>
+struct Checked {
+    T *p;
+    long long n;
+    __host__ __device__ operator T *() const { return p; }
+    // points the view at another buffer of the same length (ping-pong copies)
+    __host__ __device__ Checked &operator=(T *q)
+    {
+        p = q;
+        return *this;
+    }
+    __device__ __forceinline__ T &operator[](long long i) const
+    {
+        if (i < 0 || i >= n) {
+            if (atomicCAS(&g_ifc_bounds_err, 0, 1) == 0) atomicExch(&g_ifc_bounds_idx, (unsigned long long)i);
+            return reinterpret_cast<T *>(g_ifc_bounds_sink)[threadIdx.x & 31];
+        }
+        return p[i];
+    }
+};
+template <typename T>
+using FieldArr = Checked<T>;
+#else
+template <typename T>
+using FieldArr = T *;
+#endif
+
 template <typename T>
 struct Fields {
-    T *u, *v, *w, *p, *temp, *pc;
-    T *uf, *vf, *wf;
-    T *ac;                          // momentum diagonal after the boundary fold-in
-    T *mc, *pcoef;                  // materialised coefficient planes (2*dim+1 each)
-    T *su, *sv, *sw, *sp;           // momentum sources and p' source (mass imbalance)
-    T *tmp;                         // scratch copy for Jacobi sweeps (3*N)
-    T *rac;                         // 1/aC (3D p' sweeps)
-    T *sdc;                         // deferred-correction sources of u, v, w (dim planes; conv != 0)
+    FieldArr<T> u, v, w, p, temp, pc;
+    FieldArr<T> uf, vf, wf;
+    FieldArr<T> ac;                 // momentum diagonal after the boundary fold-in
+    FieldArr<T> mc, pcoef;          // materialised coefficient planes (2*dim+1 each)
+    FieldArr<T> su, sv, sw, sp;     // momentum sources and p' source (mass imbalance)
+    FieldArr<T> tmp;                // scratch copy for Jacobi sweeps (3*N)
+    FieldArr<T> rac;                // 1/aC (3D p' sweeps)
+    FieldArr<T> sdc;                // deferred-correction sources of u, v, w (dim planes; conv != 0)
 };
 
 struct LogRec {
@@ -79,6 +116,8 @@ struct Ctl {
     double norm[8];                 // RMS norms p u v w uf vf wf mass
     double rel[7];
     double maxn[8];                 // running maxima (criterion)
+    double res_sq[3];               // FP64 sums of squared momentum residuals (residual rule)
+    double rmax[4];                 // running maxima of the u, v, w residual and mass RMS (residual rule)
     int log_n;                      // records written by this call
     int log_level;
     LogRec log[kLogCap];

@@ -1,0 +1,255 @@
+// ifc_coop3d.cuh -- a 3D linear solve (the p' equation, or a system with
+// stored coefficients such as the temperature) as one cooperative launch,
+// with the unknown resident in shared memory and the links and source of
+// every cell packed once per solve in sweep order.
+//
+// Work split: each CTA owns a rectangular block of x-rows (all i, j in
+// [j0, j0+bj), k in [k0, k0+bk)) for the whole solve (PcBlocks, chosen on the
+// host so that one CTA per SM holds its block).  Set-up: every cell of the
+// block gets its six links -- for p' from 1/aC (kernels.cuh:518-537, FP64
+// products as in k_pc_half3d), otherwise from the stored planes -- its
+// diagonal and its source, written to a packed array in the order the sweeps
+// consume them: per (row, colour) the cells of that colour, one 16-byte
+// vector of four values per plane and cell slot.  A half sweep then reads
+// each updated cell's coefficients with two coalesced 128-bit loads and its
+// neighbours from shared memory (or, in the rows of a neighbouring block,
+// from global memory, where every CTA publishes its boundary rows after each
+// half sweep); a bounded grid barrier separates the half sweeps.  The
+// per-sweep FP64 sums are reduced by every CTA in one fixed order, so every
+// CTA takes the same inner early-exit decision (src/Solver.cu:955-962).  The
+// arithmetic of each update is that of point_update on the same
+// coefficients, so the results equal the per-half-sweep kernels and the CPU
+// oracle bit for bit.  Only the unknown takes shared memory (the source
+// travels with the links), so FP64 grids of the size FP32 ones run at fit
+// as well.
+#pragma once
+
+#include "ifc_fused3d.cuh"
+
+namespace ifc {
+
+// Four consecutive values from a 16-byte aligned address, bypassing L1 (each
+// packed value is read once per half sweep).
+__device__ __forceinline__ void ld4(const float *p, float (&o)[4])
+{
+    const float4 v = __ldcg(reinterpret_cast<const float4 *>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double (&o)[4])
+{
+    const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+template <typename T>
+__device__ __forceinline__ void st4(T *p, T a, T b, T c, T d)
+{
+    p[0] = a;
+    p[1] = b;
+    p[2] = c;
+    p[3] = d;
+}
+
+// Packed slots: per CTA rows_cap rows x 2 colours x hx cells, hx = (nx+1)/2;
+// the cell (i, row r, colour c) sits in slot (2r + c) * hx + (i >> 1) of its
+// CTA's range.  Two planes of 4 values per slot follow each other, each
+// spanning all CTAs' slots.
+__host__ __device__ inline long long coop3d_slots(const PcBlocks &B, int nx)
+{
+    return (long long)B.nbj * B.nbk * B.bj * B.bk * 2 * ((nx + 1) / 2);
+}
+
+// Shared memory: the row table (int4 per row), the boundary-row list, then
+// the unknown of every cell of the block.
+template <typename T>
+__host__ __device__ inline size_t coop3d_smem_bytes(int rows, int nx)
+{
+    return (size_t)rows * 16 + (size_t)((rows + 3) & ~3) * 4 + (size_t)rows * nx * sizeof(T);
+}
+
+// The linear system a cooperative solve works on: the p' equation (coef null:
+// links from 1/aC, start from p' = 0 without clearing the array, as the
+// per-half-sweep kernel does) or a system with stored coefficient planes
+// coef[cell + N*slot] (slots aC aE aW aN aS aT aB), e.g. the temperature.
+// Unknown x, source src, equation slot eq of the control block (relaxation,
+// tolerance, sweep bookkeeping).
+template <typename T>
+struct CSys {
+    const T *coef;
+    const T *src;
+    T *x;
+    int eq;
+};
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_csolve3d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials,
+                                                    GridBarrier *bar, PcBlocks B, int n_sweeps, T *pk, CSys<T> sys)
+{
+    const Geo<T> &g = P.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
+    const int G = gridDim.x, tid = threadIdx.x;
+    const int j0 = (blockIdx.x % B.nbj) * B.bj, k0 = (blockIdx.x / B.nbj) * B.bk;
+    const int nj = min(B.bj, ny - j0), nk = min(B.bk, nz - k0);
+    const int rows_cap = B.bj * B.bk;
+    const int nrow = nj * nk;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int ln = nx, lt = nx * nj;  // local strides to the next row in j and in k
+    const int hx = (nx + 1) / 2;
+    const long long S = coop3d_slots(B, nx);
+    const long long cbase = (long long)blockIdx.x * rows_cap * 2 * hx;
+    T *pA = pk, *pB = pk + 4 * S;  // {aC, aE, aW, aN}, {aS, aT, aB, b}
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int4 *s_row = reinterpret_cast<int4 *>(smem_raw);
+    int *s_bnd = reinterpret_cast<int *>(s_row + rows_cap);
+    T *s_x = reinterpret_cast<T *>(s_bnd + ((rows_cap + 3) & ~3));
+    __shared__ int nbnd;
+    __shared__ double red[NT / 32];
+    __shared__ double tot2[2];
+    const int eq = sys.eq;
+    const bool zero_start = sys.coef == nullptr;
+    T *x = sys.x;
+
+    // row table: x = global offset of the row, y = j, z = k, w = flags (1: row
+    // j+1 in this block, 2: j-1, 4: k+1, 8: k-1)
+    for (int r = tid; r < nrow; r += NT) {
+        const int jj = r % nj, kk = r / nj;
+        const int j = j0 + jj, k = k0 + kk;
+        const int fl = (jj + 1 < nj ? 1 : 0) | (jj > 0 ? 2 : 0) | (kk + 1 < nk ? 4 : 0) | (kk > 0 ? 8 : 0);
+        s_row[r] = make_int4(nx * (j + ny * k), j, k, fl);
+    }
+    if (tid == 0) {
+        int n = 0;
+        for (int r = 0; r < nrow; ++r) {
+            const int jj = r % nj, kk = r / nj;
+            if (jj == 0 || jj == nj - 1 || kk == 0 || kk == nk - 1) s_bnd[n++] = r;
+        }
+        nbnd = n;
+    }
+    __syncthreads();
+    // packed links and sources of the CTA's cells, the unknown into shared memory
+    for (int r = warp; r < nrow; r += NT / 32) {
+        const int4 ri = s_row[r];
+        const int j = ri.y, k = ri.z, crow = ri.x, lrow = nx * r;
+        for (int i = lane; i < nx; i += 32) {
+            const int c = crow + i;
+            T a[7];
+            if (zero_start) {
+                const T rr = f.rac[c];
+                a[AE] = i < nx - 1 ? (T)(P.d.Kx * (double)(T)(rr + f.rac[c + 1])) : (T)0;
+                a[AW] = i > 0 ? (T)(P.d.Kx * (double)(T)(rr + f.rac[c - 1])) : (T)0;
+                a[AN] = j < ny - 1 ? (T)(P.d.Ky * (double)(T)(rr + f.rac[c + nx])) : (T)0;
+                a[AS] = j > 0 ? (T)(P.d.Ky * (double)(T)(rr + f.rac[c - nx])) : (T)0;
+                a[AT] = k < nz - 1 ? (T)(P.d.Kz * (double)(T)(rr + f.rac[c + pl])) : (T)0;
+                a[AB] = k > 0 ? (T)(P.d.Kz * (double)(T)(rr + f.rac[c - pl])) : (T)0;
+                a[AC] = -(a[AE] + a[AW] + a[AN] + a[AS]);
+                a[AC] += -(a[AT] + a[AB]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 7; ++q) a[q] = sys.coef[c + (size_t)N * q];
+            }
+            const long long slot = cbase + (long long)(2 * r + ((i + j + k) & 1)) * hx + (i >> 1);
+            st4(pA + 4 * slot, a[AC], a[AE], a[AW], a[AN]);
+            st4(pB + 4 * slot, a[AS], a[AT], a[AB], sys.src[c]);
+            s_x[lrow + i] = zero_start ? (T)0 : x[c];
+        }
+    }
+    double mx = ctl->inner_max[eq];
+    int sw = ctl->sweeps[eq];
+    bool stop = ctl->stop[eq] != 0;
+    double last_sq = 0.0;
+    unsigned int epoch = 0;
+    __syncthreads();  // the packed values are read back by the same CTA only
+
+    bool failed = false;
+    for (int s = 0; s < n_sweeps && !stop && !failed; ++s) {
+        for (int color = 0; color < 2; ++color) {
+            const int zero_mode = (zero_start && s == 0) ? (color == 0 ? 1 : 2) : 0;
+            const bool zn = zero_mode == 1;
+            double sq = 0.0;
+            for (int r = warp; r < nrow; r += NT / 32) {
+                const int4 ri = s_row[r];
+                const int j = ri.y, k = ri.z;
+                const int lrow = nx * r, crow = ri.x;
+                const bool inN = ri.w & 1, inS = ri.w & 2, inT = ri.w & 4, inB = ri.w & 8;
+                const int off = (color + j + k) & 1;
+                const long long sbase = cbase + (long long)(2 * r + color) * hx;
+                for (int i = off + 2 * lane; i < nx; i += 64) {
+                    const int l = lrow + i, c = crow + i;
+                    const long long slot = sbase + (i >> 1);
+                    T q0[4], q1[4];
+                    ld4(pA + 4 * slot, q0);
+                    ld4(pB + 4 * slot, q1);
+                    const T a[7] = {q0[0], q0[1], q0[2], q0[3], q1[0], q1[1], q1[2]};
+                    const T pE = (!zn && i != nx - 1) ? s_x[l + 1] : (T)0;
+                    const T pW = (!zn && i != 0) ? s_x[l - 1] : (T)0;
+                    const T pN = (!zn && j != ny - 1) ? (inN ? s_x[l + ln] : __ldcg(&x[c + nx])) : (T)0;
+                    const T pS = (!zn && j != 0) ? (inS ? s_x[l - ln] : __ldcg(&x[c - nx])) : (T)0;
+                    const T pT = (!zn && k != nz - 1) ? (inT ? s_x[l + lt] : __ldcg(&x[c + pl])) : (T)0;
+                    const T pB_ = (!zn && k != 0) ? (inB ? s_x[l - lt] : __ldcg(&x[c - pl])) : (T)0;
+                    const T pc = zero_mode ? (T)0 : s_x[l];
+                    T d;
+                    s_x[l] = point_update<T, 3>(a, q1[3], pc, pE, pW, pN, pS, pT, pB_, g.relax[eq], d);
+                    sq += (double)d * (double)d;
+                }
+            }
+            __syncthreads();
+            // publish this colour's cells of the boundary rows
+            for (int b = warp; b < nbnd; b += NT / 32) {
+                const int r = s_bnd[b];
+                const int4 ri = s_row[r];
+                const int lrow = nx * r, crow = ri.x;
+                for (int i = ((color + ri.y + ri.z) & 1) + 2 * lane; i < nx; i += 64) x[crow + i] = s_x[lrow + i];
+            }
+            sq = warp_sum(sq);
+            if (lane == 0) red[warp] = sq;
+            __syncthreads();
+            if (tid == 0) {
+                double t = 0.0;
+                for (int w = 0; w < NT / 32; ++w) t += red[w];
+                partials[(size_t)(2 * (s & 1) + color) * G + blockIdx.x] = t;
+            }
+            if (!grid_sync(bar, G, epoch)) {
+                failed = true;
+                break;
+            }
+        }
+        if (failed) break;
+        // grid sums of both halves, fixed order, identical in every CTA
+        if (tid < 64) {
+            const int color = tid >> 5;
+            double t = 0.0;
+            for (int b = lane; b < G; b += 32) t += __ldcg(&partials[(size_t)(2 * (s & 1) + color) * G + b]);
+            t = warp_sum(t);
+            if (lane == 0) tot2[color] = t;
+        }
+        __syncthreads();
+        const double ssq = tot2[0] + tot2[1];
+        const double rms = sqrt(ssq / (double)N);
+        if (rms > mx) mx = rms;
+        if (rms / (mx + 1e-20) < g.tol[eq]) stop = true;
+        ++sw;
+        last_sq = ssq;
+        __syncthreads();  // tot2 is rewritten only after the next sweep's barriers
+    }
+    for (int r = warp; r < nrow; r += NT / 32) {
+        const int crow = s_row[r].x, lrow = nx * r;
+        for (int i = lane; i < nx; i += 32) x[crow + i] = s_x[lrow + i];
+    }
+    if (blockIdx.x == 0 && tid == 0 && !failed) {
+        const int done = sw - ctl->sweeps[eq];
+        ctl->cell_updates += (long long)done * N;
+        ctl->inner_max[eq] = mx;
+        ctl->sweeps[eq] = sw;
+        if (done > 0) ctl->last_sweep_sq[eq] = last_sq;
+        if (stop) ctl->stop[eq] = 1;
+    }
+    if (tid == 0 && (failed || bar->err)) atomicExch(&ctl->status, 3);
+}
+
+}  // namespace ifc

@@ -17,6 +17,7 @@
 #include "ifc_kernels.cuh"
 #include "ifc_persist2d.cuh"
 #include "ifc_fused3d.cuh"
+#include "ifc_coop3d.cuh"
 #include "ifc_energy.cuh"
 
 namespace ifc {
@@ -84,7 +85,7 @@ Params<T> make_params(const ifc_config &c)
         for (int q = 0; q < 3; ++q) g.bcv[f][q] = (T)c.vel_bc_val[f][q];
     }
     g.inlet = nullptr;
-    g.criterion = c.criterion == IFC_CRIT_REFERENCE ? 0 : 1;
+    g.criterion = c.criterion == IFC_CRIT_REFERENCE ? 0 : c.criterion == IFC_CRIT_RESIDUAL ? 2 : 1;
     g.conv = c.convection_scheme;
     Derived<T> &d = P.d;
     d.Dx = g.mu * g.Ax / g.dx;
@@ -133,10 +134,13 @@ struct Engine : EngineBase {
     long long launches_per_iter = 0;  // kernels in one captured outer iteration
     long long last_launches = 0;
     AdjointCtx *adj = nullptr;        // discrete-adjoint buffers and graphs (first ifc_adjoint call)
-    bool pc3d = false;                // 3D p' solve as one cooperative launch (k_pc_solve3d)
+    // The 3D p' solve as one cooperative launch (ifc_coop3d.cuh): row blocks,
+    // shared memory per CTA, and the packed links and sources
+    static constexpr int kPcNT = 1024;
+    bool pc3d = false;
     PcBlocks pcb = {0, 0, 0, 0};
     size_t pc3d_smem = 0;
-    static constexpr int kPcNT = 1024;
+    T *packed = nullptr;
 
     ~Engine() override
     {
@@ -159,6 +163,36 @@ struct Engine : EngineBase {
         if (b > max_grid) b = max_grid;
         return (int)b;
     }
+
+#ifdef IFC_BOUNDS_CHECK
+    template <typename U>
+    int alloc(Checked<U> *p, size_t n)
+    {
+        U *q = nullptr;
+        int rc = alloc(&q, n);
+        p->p = q;
+        p->n = (long long)n;
+        return rc;
+    }
+
+    // IFC_BAD_ARGUMENT when a kernel of the last launch sequence indexed a
+    // field array out of range (the flag is then cleared).
+    int bounds_status()
+    {
+        int e = 0;
+        unsigned long long idx = 0;
+        IFC_CK(cudaMemcpyFromSymbol(&e, g_ifc_bounds_err, sizeof(int)));
+        if (!e) return IFC_OK;
+        IFC_CK(cudaMemcpyFromSymbol(&idx, g_ifc_bounds_idx, sizeof(idx)));
+        const int zero = 0;
+        IFC_CK(cudaMemcpyToSymbol(g_ifc_bounds_err, &zero, sizeof(int)));
+        err = "bounds check: a kernel indexed a field array out of range (index " +
+              std::to_string((long long)idx) + ")";
+        return IFC_BAD_ARGUMENT;
+    }
+#else
+    int bounds_status() { return IFC_OK; }
+#endif
 
     template <typename U>
     int alloc(U **p, size_t n)
@@ -252,9 +286,10 @@ struct Engine : EngineBase {
         cond = 0;
     }
 
-    // Row blocks of the single-launch 3D p' solve: the smallest blocks (fewest
+    // Row blocks of the cooperative 3D p' solve: the smallest blocks (fewest
     // rows, then the shortest perimeter) whose count fits one CTA per SM and
-    // whose p' and b_p' fit the CTA's shared memory.
+    // whose p' fits the CTA's shared memory.  IFC_PC3D_OFF=1 keeps the
+    // per-half-sweep kernel (A/B timing, tests).
     int prepare_pc3d()
     {
         pc3d = false;
@@ -266,7 +301,7 @@ struct Engine : EngineBase {
         IFC_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         if (!coop) return IFC_OK;
         const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
-        const size_t per_row = 2 * sizeof(T) * (size_t)nx + 20;  // p', b_p' and the row table
+        const size_t per_row = sizeof(T) * (size_t)nx + 20;  // p' and the row table
         const long long max_rows = ((long long)optin - 4096) / (long long)per_row;
         if (max_rows < 1) return IFC_OK;
         long long best = -1, best_per = 0;
@@ -283,19 +318,23 @@ struct Engine : EngineBase {
                 }
             }
         if (best < 0) return IFC_OK;
-        const size_t smem = pc3d_smem_bytes<T>(b.bj * b.bk, nx);
-        auto kern = k_pc_solve3d<T, kPcNT>;
+        const size_t smem = coop3d_smem_bytes<T>(b.bj * b.bk, nx);
+        auto kern = k_csolve3d<T, kPcNT>;
         IFC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         IFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPcNT, smem));
         if (per_sm < 1 || (long long)per_sm * nsm < (long long)b.nbj * b.nbk) return IFC_OK;
+        int rc = alloc(&packed, (size_t)coop3d_slots(b, nx) * 8);
+        if (rc != IFC_OK) return rc;
         pcb = b;
         pc3d_smem = smem;
         pc3d = true;
         return IFC_OK;
     }
 
-    void enq_pc_solve3d()
+    // The p' solve (sys.coef null) or a stored-coefficient system as one
+    // cooperative launch of n sweeps (k_csolve3d).
+    void enq_csolve3d(const Params<T> &PP, CSys<T> sys, int n)
     {
         cudaMemsetAsync(barrier, 0, sizeof(GridBarrier), stream);
         cudaLaunchConfig_t lc = {};
@@ -308,8 +347,14 @@ struct Engine : EngineBase {
         at[0].val.cooperative = 1;
         lc.attrs = at;
         lc.numAttrs = 1;
-        cudaLaunchKernelEx(&lc, k_pc_solve3d<T, kPcNT>, P, f, ctl, partials, barrier, pcb, cfg.n_iter_p);
+        cudaLaunchKernelEx(&lc, k_csolve3d<T, kPcNT>, PP, f, ctl, partials, barrier, pcb, n, packed, sys);
         ++launches;
+    }
+
+    void enq_pc_solve3d()
+    {
+        CSys<T> sys = {nullptr, f.sp, f.pc, EQ_P};
+        enq_csolve3d(P, sys, cfg.n_iter_p);
     }
 
     int set_uniform(double u, double v, double w, double p, double t) override
@@ -561,6 +606,10 @@ struct Engine : EngineBase {
         // The boundary faces of each iteration are written by the previous
         // iteration's update kernel; run() applies them before the first.
         enq_dc_source<DIM>();
+        if (P.g.criterion == 2) {
+            k_mom_residual<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f, ctl, partials);
+            ++launches;
+        }
         enq_mom_solve<DIM>();
         enq_rhie_chow<DIM>();
         enq_pcorr_solve<DIM>();
@@ -708,6 +757,7 @@ struct Engine : EngineBase {
         IFC_CK(cudaEventElapsedTime(&ms, ev0, ev1));
         last_ms = ms;
         if ((rc = read_ctl()) != IFC_OK) return rc;
+        if ((rc = bounds_status()) != IFC_OK) return rc;
         if (cfg.log_level > 0) print_log();
         last_launches = persist ? 3 : 2 + (long long)(ctl_h.it - ctl_h.it_begin) * launches_per_iter;
         fill_stats(st);
@@ -731,7 +781,8 @@ struct Engine : EngineBase {
         else run_stage_t<3>(stage);
         IFC_CK(cudaGetLastError());
         IFC_CK(cudaStreamSynchronize(stream));
-        return read_ctl();
+        const int rc = read_ctl();
+        return rc != IFC_OK ? rc : bounds_status();
     }
 
     template <int DIM>
@@ -781,7 +832,7 @@ struct Engine : EngineBase {
         IFC_CK(cudaEventElapsedTime(&t, ev0, ev1));
         *ms = (double)t / reps;
         if (nl) *nl = (int)((launches - l0) / reps);
-        return IFC_OK;
+        return bounds_status();
     }
 
     int sweep(int eq, int n, double *sq) override
@@ -803,7 +854,7 @@ struct Engine : EngineBase {
             if (rc != IFC_OK) return rc;
             if (sq) sq[s] = ctl_h.last_sweep_sq[eq];
         }
-        return IFC_OK;
+        return bounds_status();
     }
 
     // Steady temperature on the current flow (ifc_energy.cuh): assemble the
@@ -857,7 +908,8 @@ struct Engine : EngineBase {
         // 2D: temporally blocked passes of kEnergyKS sweeps on the stored
         // coefficients (k_coef_pass2d), ping-ponging T with scratch; the
         // early-exit rule is then applied after each pass, as in the fused
-        // p' passes.  3D: one launch per colour and sweep.
+        // p' passes.  3D: one cooperative launch per cycle when the p'
+        // solve has one (k_csolve3d), else one launch per colour and sweep.
         const bool blocked = dim == 2 && fused && cfg.linear_solver == IFC_GAUSS_SEIDEL;
         constexpr int kEnergyKS = 5;
         const int gran = blocked ? kEnergyKS : 1;  // sweeps counted per early-exit check
@@ -871,6 +923,11 @@ struct Engine : EngineBase {
             const int tiles = ((g.nx + S::TX - 1) / S::TX) * ((g.ny + S::TY - 1) / S::TY);
             if (blocked && !dc && energy_coop(tiles) && max_sweeps > 0) cycle_len = max_sweeps;
         }
+        // 3D: one cooperative launch per cycle on the stored planes
+        // (k_csolve3d), the early-exit rule applied after every sweep on the
+        // device, as the per-sweep launches apply it.
+        const bool coop3 = dim == 3 && pc3d && cfg.linear_solver == IFC_GAUSS_SEIDEL;
+        if (coop3 && !dc && max_sweeps > 0) cycle_len = max_sweeps;
         int done = 0, cycle_start = 0;
         while (done < max_sweeps) {
             const int chunk = max_sweeps - done < cycle_len ? max_sweeps - done : cycle_len;
@@ -902,6 +959,9 @@ struct Engine : EngineBase {
                     cur ^= 1;
                 }
                 if (cur) IFC_CK(cudaMemcpyAsync(f.temp, tbuf[1], (size_t)N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+            } else if (coop3) {
+                CSys<T> sys = {f.mc, src_eff, f.temp, EQ_W};
+                enq_csolve3d(PT, sys, chunk);
             } else {
                 for (int q = 0; q < chunk; ++q)
                     for (int color = 0; color < 2; ++color) {
@@ -945,6 +1005,7 @@ struct Engine : EngineBase {
         }
         k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << EQ_W);
         IFC_CK(cudaStreamSynchronize(stream));
+        if ((rc = bounds_status()) != IFC_OK) return rc;
         return ctl_h.stop[EQ_W] || tol == 0.0 ? IFC_OK : IFC_NOT_CONVERGED;
     }
 

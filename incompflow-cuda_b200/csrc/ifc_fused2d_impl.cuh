@@ -231,6 +231,8 @@ int Engine<T>::prepare_persist()
     persist = false;
     persist_mt = false;
     if (dim != 2 || !fused || cfg.linear_solver != IFC_GAUSS_SEIDEL) return IFC_OK;
+    // the residual rule needs the residual pass of the graph form
+    if (P.g.criterion == 2) return IFC_OK;
     const char *off = std::getenv("IFC_PERSIST_OFF");  // the multi-kernel graph instead (A/B timing, tests)
     if (off && off[0] == '1') return IFC_OK;
     int coop = 0, dev = 0;

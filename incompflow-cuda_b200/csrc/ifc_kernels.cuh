@@ -114,6 +114,51 @@ __device__ __forceinline__ void mom_cell_global(const Params<T> &P, const Fields
     add_dc<T, DIM>(P, f, c, b);
 }
 
+// ---- FP64 momentum residuals (residual convergence rule) ------------------
+// Sum of squares of b - aC phi - sum a_nb phi_nb of each momentum component
+// at the start of the outer iteration, every product in FP64, for the
+// per-field rule on residuals (ifc_config.criterion = IFC_CRIT_RESIDUAL): in
+// FP32 the correction norms level off at the rounding noise of the corrected
+// fields, the residual of the assembled equations does not.  A library
+// addition; the reference tests its corrections only.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_mom_residual(Params<T> P, Fields<T> f, Ctl *ctl, double *partials)
+{
+    const Geo<T> &g = P.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int units = row_units(nx, ny * nz);
+    const T *phi[3] = {f.u, f.v, f.w};
+    double sq[3] = {0.0, 0.0, 0.0};
+    for (int u = gw; u < units; u += nw) {
+        const RowUnit w = row_unit(u, nx, ny);
+        const int j = w.j, k = w.k;
+        for (int i = w.i0 + lane; i < w.i1; i += 32) {
+            const int c = i + nx * w.r;
+            T a[7], b[3];
+            mom_cell_global<T, DIM>(P, f, i, j, k, a, b);
+#pragma unroll
+            for (int m = 0; m < DIM; ++m) {
+                const T *x = phi[m];
+                double r = (double)b[m] - (double)a[AC] * (double)x[c];
+                if (i < nx - 1) r -= (double)a[AE] * (double)x[c + 1];
+                if (i > 0) r -= (double)a[AW] * (double)x[c - 1];
+                if (j < ny - 1) r -= (double)a[AN] * (double)x[c + nx];
+                if (j > 0) r -= (double)a[AS] * (double)x[c - nx];
+                if (DIM == 3) {
+                    if (k < nz - 1) r -= (double)a[AT] * (double)x[c + pl];
+                    if (k > 0) r -= (double)a[AB] * (double)x[c - pl];
+                }
+                sq[m] += r * r;
+            }
+        }
+    }
+    __shared__ double tot[3];
+    if (grid_reduce<3>(sq, partials, ctl, tot) && threadIdx.x == 0)
+        for (int m = 0; m < 3; ++m) ctl->res_sq[m] = tot[m];
+}
+
 // ---- momentum assembly (materialised) ------------------------------------
 // kernels.cuh:97-134, :136-250, :252-334 for every cell; writes the coefficient
 // planes, the diagonal and the sources.
@@ -410,7 +455,26 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
 #pragma unroll
         for (int q = 0; q < 7; ++q) bad = bad || (maxn[q] > 0.0 && n[q] > 1e6 * maxn[q]);
     double rel[7];
-    if (g.criterion == 0) {
+    double rmax[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rmax[q] = ctl->rmax[q];
+    if (g.criterion == 2) {
+        // per field on the FP64 residuals: u, v, w by their momentum residual,
+        // p by the mass imbalance; the faces follow from u and p
+        const double r[4] = {sqrt(ctl->res_sq[0] / N), sqrt(ctl->res_sq[1] / N), d3 ? sqrt(ctl->res_sq[2] / N) : 0.0,
+                             n[7]};
+        double rr[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (r[q] > rmax[q]) rmax[q] = r[q];
+            rr[q] = rmax[q] > 0.0 ? r[q] / rmax[q] : 0.0;
+        }
+        rel[0] = rr[3];
+        rel[1] = rr[0];
+        rel[2] = rr[1];
+        rel[3] = d3 ? rr[2] : 0.0;
+        rel[4] = rel[5] = rel[6] = 0.0;
+    } else if (g.criterion == 0) {
         // src/Solver.cu:237-256: all relative norms use the running max of the
         // pressure norm.
         if (n[0] > maxn[0]) maxn[0] = n[0];
@@ -444,6 +508,8 @@ __device__ void finish_iteration(const Geo<T> &g, Ctl *ctl, const double *tot, c
     }
 #pragma unroll
     for (int q = 0; q < 7; ++q) ctl->rel[q] = rel[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ctl->rmax[q] = rmax[q];
     ctl->it = it;
     ctl->converged = conv ? 1 : 0;
     if (bad) ctl->status = 2;

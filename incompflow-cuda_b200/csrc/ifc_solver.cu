@@ -30,6 +30,15 @@ extern "C" {
 
 int ifc_abi_version(void) { return IFC_ABI_VERSION; }
 
+int ifc_build_flags(void)
+{
+#ifdef IFC_BOUNDS_CHECK
+    return IFC_BUILD_BOUNDS_CHECK;
+#else
+    return 0;
+#endif
+}
+
 const char *ifc_status_string(int s)
 {
     switch (s) {
@@ -98,7 +107,8 @@ int ifc_config_check(const ifc_config *c)
         return IFC_BAD_CONFIG;
     if (c->precision != IFC_FP32 && c->precision != IFC_FP64) return IFC_BAD_CONFIG;
     if (c->linear_solver != IFC_GAUSS_SEIDEL && c->linear_solver != IFC_JACOBI) return IFC_BAD_CONFIG;
-    if (c->criterion != IFC_CRIT_REFERENCE && c->criterion != IFC_CRIT_PER_FIELD) return IFC_BAD_CONFIG;
+    if (c->criterion != IFC_CRIT_REFERENCE && c->criterion != IFC_CRIT_PER_FIELD && c->criterion != IFC_CRIT_RESIDUAL)
+        return IFC_BAD_CONFIG;
     if (c->pin_pressure < -1 || c->pin_pressure > 1) return IFC_BAD_CONFIG;
     if (c->sweeps_per_pass < 0 || c->sweeps_per_pass > 16) return IFC_BAD_CONFIG;
     if (c->convection_scheme < IFC_CONV_UPWIND || c->convection_scheme > IFC_CONV_VAN_LEER) return IFC_BAD_CONFIG;

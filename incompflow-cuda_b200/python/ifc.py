@@ -21,13 +21,15 @@ import os
 import numpy as np
 
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG, "lib", "libifc.so")
+# IFC_LIB selects another build of the library, e.g. the bounds-checked
+# lib/libifc_bc.so (make -C incompflow-cuda_b200 lib_bc).
+LIB_PATH = os.environ.get("IFC_LIB") or os.path.join(PKG, "lib", "libifc.so")
 
 OK, NOT_CONVERGED, DIVERGED, TIMEOUT, CUDA_ERROR, BAD_CONFIG, BAD_ARGUMENT, IO_ERROR, UNSUPPORTED = range(9)
 EAST, WEST, NORTH, SOUTH, TOP, BOTTOM = range(6)
 WALL, INLET, OUTLET = range(3)
 GAUSS_SEIDEL, JACOBI = 0, 1
-CRIT_REFERENCE, CRIT_PER_FIELD = 0, 1
+CRIT_REFERENCE, CRIT_PER_FIELD, CRIT_RESIDUAL = 0, 1, 2
 CONV_UPWIND, CONV_CENTRAL, CONV_SOU, CONV_QUICK, CONV_MINMOD, CONV_VAN_LEER = range(6)
 CONV_NAMES = {"upwind": CONV_UPWIND, "central": CONV_CENTRAL, "sou": CONV_SOU, "quick": CONV_QUICK,
               "minmod": CONV_MINMOD, "van_leer": CONV_VAN_LEER}
@@ -134,6 +136,7 @@ EXPORTS = {
     "ifc_adjoint_apply": (C.c_int, [C.c_void_p] + [_DP] * 12),
     "ifc_set_inlet_profile": (C.c_int, [C.c_void_p, _DP]),
     "ifc_solve_energy": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(IfcEnergyResult)]),
+    "ifc_build_flags": (C.c_int, []),
 }
 
 

@@ -43,7 +43,7 @@ enum { ORC_AC = 0, ORC_AE = 1, ORC_AW = 2, ORC_AN = 3, ORC_AS = 4, ORC_AT = 5, O
 /* Linear sweep orderings. */
 enum { ORC_GS_LEX = 0, ORC_GS_REDBLACK = 1, ORC_JACOBI = 2 };
 /* Convergence rules. */
-enum { ORC_CRIT_REFERENCE = 0, ORC_CRIT_PER_FIELD = 1 };
+enum { ORC_CRIT_REFERENCE = 0, ORC_CRIT_PER_FIELD = 1, ORC_CRIT_RESIDUAL = 2 };
 /* Equation ids for the linear solves. */
 enum { ORC_EQ_U = 0, ORC_EQ_V = 1, ORC_EQ_W = 2, ORC_EQ_P = 3 };
 /* Convection schemes; every scheme but upwind is applied by deferred correction. */
@@ -63,7 +63,7 @@ typedef struct orc_config {
     double tol_mass;
     int sweep_mode;         /* ORC_GS_LEX / ORC_GS_REDBLACK / ORC_JACOBI */
     int check_every;        /* sweeps between inner early-exit checks (1 = reference) */
-    int criterion;          /* ORC_CRIT_REFERENCE / ORC_CRIT_PER_FIELD */
+    int criterion;          /* ORC_CRIT_REFERENCE / ORC_CRIT_PER_FIELD / ORC_CRIT_RESIDUAL */
     int pin_pressure;       /* subtract the FP64 mean of p' (closed domains) */
     const double *inlet_profile; /* optional: west-face normal velocity per boundary cell (ny*nz) */
     int convection;         /* ORC_CONV_*; 0 = first-order upwind, the reference's only scheme */
@@ -73,6 +73,7 @@ typedef struct orc_config {
 typedef struct orc_norms {
     double p, u, v, w, uf, vf, wf, mass;
     double rel_p, rel_u, rel_v, rel_w, rel_uf, rel_vf, rel_wf;
+    double res_u, res_v, res_w;  /* RMS momentum residuals at the start of the iteration (FP64) */
     int sweeps[4];          /* sweeps actually done in this outer iteration */
     int converged;
 } orc_norms;

@@ -26,6 +26,7 @@ struct CAT(orc_state_, S) {
     T *tmp;
     int it;
     double max_p, max_u, max_v, max_w, max_uf, max_vf, max_wf;
+    double rmax[4];             /* running maxima of the u, v, w residuals and the mass imbalance */
 };
 
 #define CID(s, i, j, k) ((size_t)(i) + (size_t)(s)->nx * ((size_t)(j) + (size_t)(s)->ny * (size_t)(k)))
@@ -651,6 +652,36 @@ void FN(update_field)(ST *s, orc_norms *out)
     }
 }
 
+/* Sum of squares, in FP64, of the residual b - aC phi - sum a_nb phi_nb of
+ * the assembled momentum equation of component `eq` at the current field
+ * (out-of-domain neighbours enter as 0, as in the sweeps).  A library
+ * addition: the reference measures convergence by its corrections only. */
+static double FN(mom_residual_sq)(ST *s, int eq)
+{
+    const T *a = s->f[ORC_F_MCOEF];
+    const T *b = s->f[eq == ORC_EQ_U ? ORC_F_SRC_U : eq == ORC_EQ_V ? ORC_F_SRC_V : ORC_F_SRC_W];
+    const T *x = s->f[eq == ORC_EQ_U ? ORC_F_U : eq == ORC_EQ_V ? ORC_F_V : ORC_F_W];
+    const size_t N = s->N;
+    double sum = 0.0;
+    for (int k = 0; k < s->nz; ++k)
+        for (int j = 0; j < s->ny; ++j)
+            for (int i = 0; i < s->nx; ++i) {
+                const size_t c = CID(s, i, j, k);
+                double r = (double)b[c] - (double)a[c + N * ORC_AC] * (double)x[c];
+                if (i < s->nx - 1) r -= (double)a[c + N * ORC_AE] * (double)x[c + 1];
+                if (i > 0) r -= (double)a[c + N * ORC_AW] * (double)x[c - 1];
+                if (j < s->ny - 1) r -= (double)a[c + N * ORC_AN] * (double)x[c + s->nx];
+                if (j > 0) r -= (double)a[c + N * ORC_AS] * (double)x[c - s->nx];
+                if (s->dim == 3) {
+                    const size_t pl = (size_t)s->nx * s->ny;
+                    if (k < s->nz - 1) r -= (double)a[c + N * ORC_AT] * (double)x[c + pl];
+                    if (k > 0) r -= (double)a[c + N * ORC_AB] * (double)x[c - pl];
+                }
+                sum += r * r;
+            }
+    return sum;
+}
+
 /* One SIMPLE outer iteration, src/Solver.cu:160-289, followed by the norms and
  * the convergence test.  Returns 1 when converged. */
 int FN(outer_iteration)(ST *s, orc_norms *out)
@@ -663,6 +694,11 @@ int FN(outer_iteration)(ST *s, orc_norms *out)
     FN(mom_src)(s);
     FN(bc_mom)(s);
     FN(dc_source)(s);
+    if (s->cfg.criterion == ORC_CRIT_RESIDUAL) {
+        nm.res_u = sqrt(FN(mom_residual_sq)(s, ORC_EQ_U) / (double)s->N);
+        nm.res_v = sqrt(FN(mom_residual_sq)(s, ORC_EQ_V) / (double)s->N);
+        if (s->dim == 3) nm.res_w = sqrt(FN(mom_residual_sq)(s, ORC_EQ_W) / (double)s->N);
+    }
     nm.sweeps[ORC_EQ_U] = FN(linear_solve)(s, ORC_EQ_U, NULL);
     nm.sweeps[ORC_EQ_V] = FN(linear_solve)(s, ORC_EQ_V, NULL);
     if (s->dim == 3) nm.sweeps[ORC_EQ_W] = FN(linear_solve)(s, ORC_EQ_W, NULL);
@@ -695,11 +731,23 @@ int FN(outer_iteration)(ST *s, orc_norms *out)
         nm.rel_p = nm.p / mx; nm.rel_u = nm.u / mx; nm.rel_v = nm.v / mx;
         nm.rel_uf = nm.uf / mx; nm.rel_vf = nm.vf / mx;
         nm.rel_w = nm.w / mx; nm.rel_wf = nm.wf / mx;
-    } else {
+    } else if (s->cfg.criterion == ORC_CRIT_PER_FIELD) {
 #define RELF(x) do { if (nm.x > s->max_##x) s->max_##x = nm.x; nm.rel_##x = s->max_##x > 0 ? nm.x / s->max_##x : 0.0; } while (0)
         RELF(p); RELF(u); RELF(v); RELF(uf); RELF(vf);
         if (s->dim == 3) { RELF(w); RELF(wf); }
 #undef RELF
+    } else {
+        /* Per field on the FP64 residuals: u, v, w by their momentum residual,
+         * p by the mass imbalance, each over its own running maximum; the
+         * face velocities follow from u and p and are not tested. */
+        const double r[4] = {nm.res_u, nm.res_v, nm.res_w, nm.mass};
+        double rel[4];
+        for (int q = 0; q < 4; ++q) {
+            if (r[q] > s->rmax[q]) s->rmax[q] = r[q];
+            rel[q] = s->rmax[q] > 0 ? r[q] / s->rmax[q] : 0.0;
+        }
+        nm.rel_u = rel[0]; nm.rel_v = rel[1]; nm.rel_w = s->dim == 3 ? rel[2] : 0.0; nm.rel_p = rel[3];
+        nm.rel_uf = nm.rel_vf = nm.rel_wf = 0.0;
     }
     /* src/Solver.cu:258-268 */
     int conv = nm.rel_p < (double)s->tol[ORC_EQ_P] && nm.rel_u < (double)s->tol[ORC_EQ_U] &&

@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libifc_oracle.so")
 
 GS_LEX, GS_REDBLACK, JACOBI = 0, 1, 2
-CRIT_REFERENCE, CRIT_PER_FIELD = 0, 1
+CRIT_REFERENCE, CRIT_PER_FIELD, CRIT_RESIDUAL = 0, 1, 2
 EQ_U, EQ_V, EQ_W, EQ_P = 0, 1, 2, 3
 # Convection schemes (0 is the reference's first-order upwind; the others are
 # applied by deferred correction).
@@ -46,7 +46,8 @@ class OrcConfig(C.Structure):
 
 class OrcNorms(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("p", "u", "v", "w", "uf", "vf", "wf", "mass",
-                                           "rel_p", "rel_u", "rel_v", "rel_w", "rel_uf", "rel_vf", "rel_wf")] + [
+                                           "rel_p", "rel_u", "rel_v", "rel_w", "rel_uf", "rel_vf", "rel_wf",
+                                           "res_u", "res_v", "res_w")] + [
         ("sweeps", C.c_int * 4), ("converged", C.c_int)]
 
     def as_dict(self):

@@ -72,3 +72,18 @@ def test_null_arguments():
     assert lib.ifc_destroy(None) == ifc.OK
     assert lib.ifc_solve(None, None) == ifc.BAD_ARGUMENT
     assert lib.ifc_status_string(ifc.DIVERGED) == b"diverged"
+
+
+def test_bounds_checked_build_exports_the_same_symbols():
+    """lib/libifc_bc.so (make lib_bc) is the same C ABI with index checks in
+    its kernels; ifc_build_flags tells the two builds apart."""
+    path = os.path.join(ROOT, "incompflow-cuda_b200", "lib", "libifc_bc.so")
+    if not os.path.exists(path):
+        import subprocess
+
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "incompflow-cuda_b200"), "lib_bc"], check=True)
+    bc = C.CDLL(path)
+    missing = [n for n in declared_functions() if not hasattr(bc, n)]
+    assert not missing, missing
+    assert bc.ifc_build_flags() == 1
+    assert ifc.load().ifc_build_flags() == 0

@@ -167,3 +167,22 @@ def test_device_3d_matches_fp64_golden(gpu_ok):
         if k == "p":
             a, b = a - a.mean(), b - b.mean()
         assert rel_l2(a, b) < 1e-4, (k, rel_l2(a, b))
+
+
+@pytest.mark.parametrize("name", ["cavity32", "channel64x16", "cavity3d12"])
+def test_residual_rule_matches_oracle(gpu_ok, name):
+    """criterion = RESIDUAL (the per-field rule on FP64 momentum residuals and
+    the mass imbalance): the device stops within two outer iterations of the
+    oracle's restatement and its fields agree to 1e-6."""
+    cfg = {"cavity32": ifc.cavity2d(32), "channel64x16": ifc.channel2d(64, 16),
+           "cavity3d12": ifc.cavity3d(12)}[name]
+    cfg = dict(cfg, criterion=ifc.CRIT_RESIDUAL)
+    s = ifc.Solver(cfg)
+    st = s.solve()
+    assert st["status"] == ifc.OK and st["converged"], st
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    n, nm = o.solve()
+    assert nm["converged"]
+    assert abs(st["outer_iterations"] - n) <= 2, (st["outer_iterations"], n)
+    for k in ("u", "v", "w") if cfg["dim"] == 3 else ("u", "v"):
+        assert rel_l2(s.get(k), o.field(k)) < 1e-6, k

@@ -80,3 +80,33 @@ def test_converged_cavity_orderings_and_precisions_agree():
     u = res[(O.GS_REDBLACK, "f")][0].reshape(64, 64)
     # Re=100 cavity, first-order upwind on 64^2: min u on the vertical centre line
     assert -0.25 < u[:, 31:33].min() < -0.19
+
+
+def test_residual_rule_restatement():
+    """The residual rule of the oracle: the FP64 momentum residual it reports is
+    the residual of the assembled equations at the iteration's starting field
+    (recomputed here with numpy from the coefficient planes), and a 24^2
+    cavity stopped by it agrees with the per-field rule's answer to 1e-4."""
+    cfg = dict(ifc.cavity2d(24), criterion=O.CRIT_RESIDUAL)
+    o = O.Oracle(to_oracle_cfg(cfg), "d")
+    o.solve(30)
+    u0, v0 = o.field("u").copy(), o.field("v").copy()
+    nm = o.outer_iteration()
+    # the coefficients of that iteration are still in the planes
+    N = 24 * 24
+    a = o.field("mcoef").reshape(5, N)
+    for x, b, res in ((u0, o.field("src_u"), nm["res_u"]), (v0, o.field("src_v"), nm["res_v"])):
+        X = x.reshape(24, 24)
+        E = np.zeros_like(X); E[:, :-1] = X[:, 1:]
+        W = np.zeros_like(X); W[:, 1:] = X[:, :-1]
+        Nn = np.zeros_like(X); Nn[:-1, :] = X[1:, :]
+        S = np.zeros_like(X); S[1:, :] = X[:-1, :]
+        r = b - a[0] * x - a[1] * E.ravel() - a[2] * W.ravel() - a[3] * Nn.ravel() - a[4] * S.ravel()
+        assert abs(np.sqrt(np.mean(r ** 2)) - res) <= 1e-12 * max(res, 1e-300) + 1e-300
+    o2 = O.Oracle(to_oracle_cfg(cfg), "d")
+    n, nm2 = o2.solve()
+    assert nm2["converged"]
+    o3 = O.Oracle(to_oracle_cfg(dict(cfg, criterion=O.CRIT_PER_FIELD)), "d")
+    o3.solve()
+    for k in ("u", "v"):
+        assert rel_l2(o2.field(k), o3.field(k)) < 1e-4, k
