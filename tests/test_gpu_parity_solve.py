@@ -186,3 +186,22 @@ def test_residual_rule_matches_oracle(gpu_ok, name):
     assert abs(st["outer_iterations"] - n) <= 2, (st["outer_iterations"], n)
     for k in ("u", "v", "w") if cfg["dim"] == 3 else ("u", "v"):
         assert rel_l2(s.get(k), o.field(k)) < 1e-6, k
+
+
+def test_3d_pcorr_inner_exit_matches_oracle(gpu_ok):
+    """The cooperative 3D p' solve with an inner tolerance loose enough that the
+    early-exit rule (src/Solver.cu:955-962) fires after about 30 of the 40
+    sweeps, decided on the device by every CTA from the same fixed-order FP64
+    sums: four outer iterations must equal the oracle bit for bit, with the
+    same number of p' sweeps."""
+    from helpers import assert_bitwise
+
+    cfg = dict(ifc.cavity3d(10, nx=12, ny=9, nz=10), nIter_p=40, tol_p=0.2)
+    s = ifc.Solver(cfg)
+    st = s.iterate(4)
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    n, nm = o.solve(4)
+    o.bc_face_vel()
+    assert 0 < st["sweeps"][3] < 40 and st["sweeps"][3] == nm["sweeps"][3], (st["sweeps"], nm["sweeps"])
+    for k in ("u", "v", "w", "p", "uf", "vf", "wf"):
+        assert_bitwise(s.get(k), o.field(k), k)
