@@ -156,6 +156,33 @@ struct Engine : EngineBase {
     // Blocks of 256 threads for the row-segment kernels (one warp per unit).
     int row_grid() const { return grid(32LL * row_units(P.g.nx, P.g.ny * P.g.nz)); }
 
+    // At most one resident wave of kernel `kern` (256 threads, no dynamic
+    // shared memory): the grid-stride kernels then run without a partial
+    // second wave, and their last-block reduction sums fewer partials.
+    // IFC_WAVE_GRID=0 keeps the plain sizing (A/B timing).
+    std::vector<std::pair<const void *, int>> wave_cap;
+    int wave_grid(const void *kern, int blocks)
+    {
+        static const bool off = [] {
+            const char *e = std::getenv("IFC_WAVE_GRID");
+            return e && e[0] == '0';
+        }();
+        if (off) return blocks;
+        int cap = -1;
+        for (auto &kv : wave_cap)
+            if (kv.first == kern) cap = kv.second;
+        if (cap < 0) {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess) {
+                cudaGetLastError();
+                per_sm = 0;
+            }
+            cap = per_sm * nsm;
+            wave_cap.push_back({kern, cap});
+        }
+        return cap > 0 && cap < blocks ? cap : blocks;
+    }
+
     int grid(long long work) const
     {
         long long b = (work + 255) / 256;
@@ -494,7 +521,7 @@ struct Engine : EngineBase {
     void enq_dc_source()
     {
         if (P.g.conv == CONV_UPWIND) return;
-        k_dc_source<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f);
+        k_dc_source<T, DIM><<<wave_grid((const void *)k_dc_source<T, DIM>, row_grid()), 256, 0, stream>>>(P, f);
         ++launches;
     }
 
@@ -522,7 +549,7 @@ struct Engine : EngineBase {
                 h.first = s == 0;
                 for (int color = 0; color < 2; ++color) {
                     h.color = color;
-                    k_mom_half3d<T><<<grid(half), 256, 0, stream>>>(P, f, ctl, partials, h);
+                    k_mom_half3d<T><<<wave_grid((const void *)k_mom_half3d<T>, grid(half)), 256, 0, stream>>>(P, f, ctl, partials, h);
                     ++launches;
                 }
             }
@@ -543,8 +570,8 @@ struct Engine : EngineBase {
             enq_fused_rc();
             return;
         }
-        k_rhie_chow<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f);
-        k_pcorr_src<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f, ctl, partials);
+        k_rhie_chow<T, DIM><<<wave_grid((const void *)k_rhie_chow<T, DIM>, row_grid()), 256, 0, stream>>>(P, f);
+        k_pcorr_src<T, DIM><<<wave_grid((const void *)k_pcorr_src<T, DIM>, row_grid()), 256, 0, stream>>>(P, f, ctl, partials);
         launches += 2;
     }
 
@@ -574,7 +601,7 @@ struct Engine : EngineBase {
             for (int s = 0; s < cfg.n_iter_p; ++s)
                 for (int color = 0; color < 2; ++color) {
                     const int zm = s == 0 ? (color == 0 ? 1 : 2) : 0;
-                    k_pc_half3d<T><<<grid(half), 256, 0, stream>>>(P, f, f.rac, ctl, partials, color, zm);
+                    k_pc_half3d<T><<<wave_grid((const void *)k_pc_half3d<T>, grid(half)), 256, 0, stream>>>(P, f, f.rac, ctl, partials, color, zm);
                     ++launches;
                 }
         } else {
@@ -596,7 +623,7 @@ struct Engine : EngineBase {
     template <int DIM>
     void enq_update(int use_cond)
     {
-        k_update<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f, ctl, partials, cond, use_cond);
+        k_update<T, DIM><<<wave_grid((const void *)k_update<T, DIM>, row_grid()), 256, 0, stream>>>(P, f, ctl, partials, cond, use_cond);
         ++launches;
     }
 
@@ -607,7 +634,7 @@ struct Engine : EngineBase {
         // iteration's update kernel; run() applies them before the first.
         enq_dc_source<DIM>();
         if (P.g.criterion == 2) {
-            k_mom_residual<T, DIM><<<row_grid(), 256, 0, stream>>>(P, f, ctl, partials);
+            k_mom_residual<T, DIM><<<wave_grid((const void *)k_mom_residual<T, DIM>, row_grid()), 256, 0, stream>>>(P, f, ctl, partials);
             ++launches;
         }
         enq_mom_solve<DIM>();
