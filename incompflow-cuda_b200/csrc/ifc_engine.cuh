@@ -161,13 +161,14 @@ struct Engine : EngineBase {
     // second wave, and their last-block reduction sums fewer partials.
     // IFC_WAVE_GRID=0 keeps the plain sizing (A/B timing).
     std::vector<std::pair<const void *, int>> wave_cap;
+    int wave_off = -1;  // IFC_WAVE_GRID, read at the handle's first launch
     int wave_grid(const void *kern, int blocks)
     {
-        static const bool off = [] {
+        if (wave_off < 0) {
             const char *e = std::getenv("IFC_WAVE_GRID");
-            return e && e[0] == '0';
-        }();
-        if (off) return blocks;
+            wave_off = (e && e[0] == '0') ? 1 : 0;
+        }
+        if (wave_off) return blocks;
         int cap = -1;
         for (auto &kv : wave_cap)
             if (kv.first == kern) cap = kv.second;
