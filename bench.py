@@ -416,8 +416,10 @@ def precision_summary(n: int) -> dict:
 def batch_summary(every: int) -> dict:
     """The seeded 256-case cavity batch in one batched solve, against the plain
     per-case loop timed on every `every`-th case (sum of per-case device times)
-    and scaled to 256 cases; the batched fields of the sampled cases are
-    compared with the plain solves'."""
+    and scaled to all 256 by cell-iterations (cells x outer iterations of each
+    case, from the batched solve, which takes the same iterations): the plain
+    loop's time per cell-iteration of the sample times the batch's total.  The
+    batched fields of the sampled cases are compared with the plain solves'."""
     import ifc
 
     cases = ifc.batch_cases(256, seed=0)
@@ -433,11 +435,13 @@ def batch_summary(every: int) -> dict:
         for f in ("u", "v"):
             worst = max(worst, rel_l2(fields[q][f], s.get(f)))
         s.close()
-    plain_est = plain_ms * len(cases) / len(sample)
+    work = [r["outer_iterations"] * c["nx"] * c["ny"] for r, c in zip(res, cases)]
+    plain_est = plain_ms * sum(work) / sum(work[q] for q in sample)
     return {"workload": "batch_cavity2d_256", "cases": len(cases),
             "solves_per_s": len(cases) / (bms * 1e-3), "batch_ms": bms,
             "plain_loop": {"cases_timed": len(sample), "which": f"every {every}th case", "device_ms": plain_ms,
                            "device_ms_scaled_to_all": plain_est,
+                           "scaling": "by cell-iterations: sum over all cases / sum over the sampled cases",
                            "solves_per_s": len(sample) / (plain_ms * 1e-3)},
             "speedup_vs_plain": plain_est / bms,
             "converged": {"batch": int(sum(r["converged"] for r in res)), "of": len(cases),
