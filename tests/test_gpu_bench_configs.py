@@ -100,7 +100,7 @@ def test_cavity128_fp32_residuals_and_accuracy(gpu_ok):
     cavity, 3000 outer iterations from rest: the u-momentum residual and the
     mass imbalance have fallen below 1e-5 of their largest values, v and w
     below 1e-4 (in FP32 these two level off near 3e-5 and 1e-5: the rounding of
-    the stored pressure sets their floor), and the fields lie within 1e-4 of
+    the stored fields sets their floor), and the fields lie within 1e-4 of
     the FP64 build after the same iterations, whose residuals keep falling."""
     cfg = dict(ifc.cavity3d(128, re=400.0), criterion=ifc.CRIT_RESIDUAL)
     s32 = ifc.Solver(dict(cfg, precision="f"))
