@@ -56,7 +56,7 @@ def parse():
                     help="skip the compact precision / batch / adjoint records of the default line")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--form", default="plain",
-                    choices=["plain", "adjoint", "precision", "batch", "convergence", "energy"],
+                    choices=["plain", "adjoint", "precision", "batch", "convergence", "energy", "slabs"],
                     help="plain: the headline throughput line; adjoint: the differentiation form")
     ap.add_argument("--profiles", type=int, default=32, help="adjoint form: seeded inlet profiles")
     ap.add_argument("--fd-profiles", type=int, default=1,
@@ -947,6 +947,89 @@ def run_energy(args):
     s.close()
 
 
+SLAB_WORKLOADS = (
+    # (name, config, slab counts, sweeps per exchange, outer iterations timed)
+    ("channel2d_4096x2048", lambda ifc: ifc.channel2d(4096, 2048), (2, 4), None, 6),
+    ("cavity3d_128x128x512", lambda ifc: ifc.cavity3d(128, nz=512), (2, 4), 4, 3),
+)
+
+
+def run_slabs(args):
+    """Slab decomposition on one GPU (ifc_slabs): each workload's grid solved
+    whole (ifc_iterate, and the same steps one stage at a time) and cut into
+    2 and 4 overlapping slabs whose halos are refreshed by device copies after
+    every step.  The slabs share one device, so their time is the sum of the
+    slabs' steps, the halo copies and the host's step-by-step orchestration:
+    the cost of the decomposition itself, the part a multi-GPU run adds to
+    each GPU's share of the work.  Each decomposed solve is checked bit for
+    bit against the whole grid's after the same iterations."""
+    import numpy as np
+    import torch
+
+    import ifc
+    import ifc_slabs as S
+
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    records = {}
+    clocks = ClockSampler(local)
+    clocks.start()
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(n)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / n
+
+    for name, make, counts, k, n in SLAB_WORKLOADS:
+        cfg = make(ifc)
+        dim = cfg["dim"]
+        sweeps = cfg["nIter_u"] + cfg["nIter_v"] + (cfg["nIter_w"] if dim == 3 else 0) + cfg["nIter_p"]
+        cells = cfg["nx"] * cfg["ny"] * (cfg["nz"] if dim == 3 else 1)
+        warm = max(args.warmup, 1)
+        whole_cfg = dict(cfg, tol_u=0.0, tol_v=0.0, tol_w=0.0, tol_p=0.0, tol_mass=0.0, pin_pressure=0)
+        s = ifc.Solver(whole_cfg)
+        s.iterate(warm)
+        ms_whole = timed(s.iterate, n)
+        ref_u = s.get("u")
+        s.close()
+        rec = {"cells": cells, "sweeps_per_outer": sweeps, "outer_iterations_timed": n,
+               "sweeps_per_exchange": k or "whole stages",
+               "whole_ifc_iterate_ms_per_outer": ms_whole}
+        for parts in (1,) + tuple(counts):
+            with S.SlabSolver(cfg, parts=parts, sweeps_per_exchange=k) as ss:
+                ss.iterate(warm)
+                x0 = ss.exchanges
+                b0 = ss.halo.bytes if ss.halo is not None else 0
+                ms = timed(ss.iterate, n)
+                exact = bool(np.array_equal(ss.gather("u"), ref_u))
+                held = sum(g1 - g0 for g0, g1 in ss.plan.span)
+                key = "stages_1_slab" if parts == 1 else f"slabs_{parts}"
+                rec[key] = {"ms_per_outer": ms, "cell_updates_per_s": cells * sweeps / (ms * 1e-3),
+                            "halo_rows": ss.plan.halo, "rows_held_over_rows": held / ss.plan.cells,
+                            "exchanges_per_outer": (ss.exchanges - x0) / n,
+                            "halo_bytes_per_outer": ((ss.halo.bytes if ss.halo is not None else 0) - b0) / n,
+                            "bitwise_equal_to_whole": exact}
+        records[name] = rec
+    clk = clocks.stop()
+    base = records[SLAB_WORKLOADS[0][0]]
+    line = {
+        "metric": METRIC, "value": base["slabs_4"]["cell_updates_per_s"], "unit": METRIC, "n_gpus": 1,
+        "steps": n, "warmup": args.warmup, "ms_per_step": base["slabs_4"]["ms_per_outer"],
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: flows from rest",
+        "config": {"workload": "slabs: " + ", ".join(w[0] for w in SLAB_WORKLOADS),
+                   "headline_value": "channel2d_4096x2048 in 4 slabs on one GPU",
+                   "timing": "host wall clock around synchronised outer iterations (the slabs' steps are host-orchestrated)"},
+        "records": records,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_convergence(args):
     """Time to convergence on the 64^2 lid-driven cavity (Re 100, alpha
     0.7/0.3, GS 5/5/50, tolerance 1e-5, from rest): this library under the
@@ -1075,6 +1158,8 @@ def main():
         run_convergence(args)
     elif args.form == "energy":
         run_energy(args)
+    elif args.form == "slabs":
+        run_slabs(args)
     else:
         run_ours(args)
 

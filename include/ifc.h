@@ -116,6 +116,12 @@ typedef struct ifc_config {
     void *stream;                     /* cudaStream_t to run on, or NULL for a private stream */
     int convection_scheme;            /* IFC_CONV_* (default IFC_CONV_UPWIND); ifc_adjoint takes
                                          IFC_CONV_UPWIND only */
+    int slab_axis_cells;              /* 0 (default): the handle holds the whole grid.  > 0: it
+                                         holds a slab of whole rows (2D) or planes (3D) of a grid
+                                         with this many cells along y (2D) or z (3D), whose
+                                         extents are ymin..ymax (zmin..zmax); that axis's spacing
+                                         is (max - min) / slab_axis_cells, bit for bit the whole
+                                         grid's.  Used by the slab decomposition; batches take 0 */
 } ifc_config;
 
 typedef struct ifc_stats {
@@ -201,7 +207,8 @@ typedef struct ifc_batch_result {
 
 /* Solves n independent 2D cases (each a full ifc_config: its own grid, fluid,
  * boundary conditions and iteration counts; all 2D, Gauss-Seidel, one
- * precision) to convergence or num_outer_iter, in persistent kernels of
+ * precision, criterion other than IFC_CRIT_RESIDUAL, slab_axis_cells 0:
+ * IFC_UNSUPPORTED otherwise) to convergence or num_outer_iter, in persistent kernels of
  * thread-block clusters that take cases from a device queue, relaunched by a
  * CUDA graph until every case has finished.  Each case runs the same SIMPLE
  * iteration as ifc_solve.  A case's size class (up to 64^2, 160^2, larger

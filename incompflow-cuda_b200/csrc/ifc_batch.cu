@@ -834,7 +834,7 @@ extern "C" int ifc_batch_solve(const ifc_config *cases, int n, ifc_batch_result 
         const int rc = ifc_config_check(&cases[c]);
         if (rc != IFC_OK) return rc;
         if (cases[c].dim != 2 || cases[c].linear_solver != IFC_GAUSS_SEIDEL || cases[c].precision != prec ||
-            cases[c].criterion == IFC_CRIT_RESIDUAL)
+            cases[c].criterion == IFC_CRIT_RESIDUAL || cases[c].slab_axis_cells != 0)
             return IFC_UNSUPPORTED;
     }
     try {

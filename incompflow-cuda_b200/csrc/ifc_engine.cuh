@@ -65,8 +65,11 @@ Params<T> make_params(const ifc_config &c)
     const T xmax = (T)c.xmax, xmin = (T)c.xmin, ymax = (T)c.ymax, ymin = (T)c.ymin;
     const T zmax = (T)c.zmax, zmin = (T)c.zmin;
     g.dx = (xmax - xmin) / (T)g.nx;
-    g.dy = (ymax - ymin) / (T)g.ny;
-    g.dz = (zmax - zmin) / (T)g.nz;
+    // A slab handle takes the whole grid's spacing along its cut axis.
+    const int sy = (c.slab_axis_cells > 0 && c.dim == 2) ? c.slab_axis_cells : g.ny;
+    const int sz = (c.slab_axis_cells > 0 && c.dim == 3) ? c.slab_axis_cells : g.nz;
+    g.dy = (ymax - ymin) / (T)sy;
+    g.dz = (zmax - zmin) / (T)sz;
     g.Ax = g.dy * g.dz;
     g.Ay = g.dz * g.dx;
     g.Az = g.dx * g.dy;

@@ -112,6 +112,7 @@ int ifc_config_check(const ifc_config *c)
     if (c->pin_pressure < -1 || c->pin_pressure > 1) return IFC_BAD_CONFIG;
     if (c->sweeps_per_pass < 0 || c->sweeps_per_pass > 16) return IFC_BAD_CONFIG;
     if (c->convection_scheme < IFC_CONV_UPWIND || c->convection_scheme > IFC_CONV_VAN_LEER) return IFC_BAD_CONFIG;
+    if (c->slab_axis_cells != 0 && c->slab_axis_cells < (c->dim == 2 ? c->ny : nz)) return IFC_BAD_CONFIG;
     return IFC_OK;
 }
 

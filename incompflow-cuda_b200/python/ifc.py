@@ -55,7 +55,7 @@ class IfcConfig(C.Structure):
         ("precision", C.c_int), ("linear_solver", C.c_int), ("criterion", C.c_int),
         ("pin_pressure", C.c_int), ("sweeps_per_pass", C.c_int), ("log_level", C.c_int),
         ("inlet_profile", C.POINTER(C.c_double)), ("stream", C.c_void_p),
-        ("convection_scheme", C.c_int),
+        ("convection_scheme", C.c_int), ("slab_axis_cells", C.c_int),
     ]
 
 
@@ -262,6 +262,7 @@ def make_struct(cfg: dict) -> tuple[IfcConfig, object]:
     c.convection_scheme = CONV_NAMES[conv] if isinstance(conv, str) else int(conv)
     if cfg.get("stream"):
         c.stream = C.c_void_p(int(cfg["stream"]))
+    c.slab_axis_cells = int(cfg.get("slab_axis_cells", 0))
     keep = None
     if cfg.get("inlet_profile") is not None:
         keep = np.ascontiguousarray(cfg["inlet_profile"], dtype=np.float64)

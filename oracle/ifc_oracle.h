@@ -67,6 +67,9 @@ typedef struct orc_config {
     int pin_pressure;       /* subtract the FP64 mean of p' (closed domains) */
     const double *inlet_profile; /* optional: west-face normal velocity per boundary cell (ny*nz) */
     int convection;         /* ORC_CONV_*; 0 = first-order upwind, the reference's only scheme */
+    int slab_axis_cells;    /* > 0: this state holds a slab of a grid with that many cells along
+                               y (2D) or z (3D); the axis spacing is the whole grid's (the
+                               library's ifc_config field of the same name) */
 } orc_config;
 
 /* Per-outer-iteration norms (RMS, FP64), src/Solver.cu:226-235. */

@@ -52,8 +52,10 @@ ST *FN(create)(const orc_config *cfg)
         T xmax = (T)cfg->xmax, xmin = (T)cfg->xmin, ymax = (T)cfg->ymax, ymin = (T)cfg->ymin;
         T zmax = (T)cfg->zmax, zmin = (T)cfg->zmin;
         s->dx = (xmax - xmin) / (T)s->nx;
-        s->dy = (ymax - ymin) / (T)s->ny;
-        s->dz = (zmax - zmin) / (T)s->nz;
+        const int sy = (cfg->slab_axis_cells > 0 && s->dim == 2) ? cfg->slab_axis_cells : s->ny;
+        const int sz = (cfg->slab_axis_cells > 0 && s->dim == 3) ? cfg->slab_axis_cells : s->nz;
+        s->dy = (ymax - ymin) / (T)sy;
+        s->dz = (zmax - zmin) / (T)sz;
         s->Ax = s->dy * s->dz;
         s->Ay = s->dz * s->dx;
         s->Az = s->dx * s->dy;

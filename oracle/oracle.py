@@ -40,7 +40,7 @@ class OrcConfig(C.Structure):
         ("relax", C.c_double * 4), ("tol", C.c_double * 4), ("tol_mass", C.c_double),
         ("sweep_mode", C.c_int), ("check_every", C.c_int), ("criterion", C.c_int),
         ("pin_pressure", C.c_int), ("inlet_profile", C.POINTER(C.c_double)),
-        ("convection", C.c_int),
+        ("convection", C.c_int), ("slab_axis_cells", C.c_int),
     ]
 
 
@@ -130,6 +130,7 @@ def make_struct(cfg: dict) -> tuple[OrcConfig, object]:
     c.pin_pressure = int(cfg.get("pin_pressure", 0))
     conv = cfg.get("convection_scheme", 0)
     c.convection = CONV[conv] if isinstance(conv, str) else int(conv)
+    c.slab_axis_cells = int(cfg.get("slab_axis_cells", 0))
     keep = None
     prof = cfg.get("inlet_profile")
     if prof is not None:
@@ -159,7 +160,7 @@ class Oracle:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             self._fn("destroy")(h)
             self._h = None
 
