@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
-                    help="skip the compact precision / batch / adjoint records of the default line")
+                    help="skip the compact precision / batch / adjoint / slabs records of the default line")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--form", default="plain",
                     choices=["plain", "adjoint", "precision", "batch", "convergence", "energy", "slabs"],
@@ -336,7 +336,8 @@ def run_ours(args):
         if world == 1 and not args.no_forms and CONVECTION == "upwind":
             forms = {}
             for name, fn in (("precision", lambda: precision_summary(args.n3d)),
-                             ("batch", lambda: batch_summary(4)), ("adjoint", lambda: adjoint_summary(4, 8))):
+                             ("batch", lambda: batch_summary(4)), ("adjoint", lambda: adjoint_summary(4, 8)),
+                             ("slabs", slabs_summary)):
                 t0 = time.perf_counter()
                 try:
                     forms[name] = fn()
@@ -351,9 +352,9 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-# ---- compact records of the three further forms in the default line --------
+# ---- compact records of the further forms in the default line --------------
 # Each runs after the headline's timed region, on rank 0 at N = 1, and takes
-# seconds; the full forms are bench.py --form precision|batch|adjoint.
+# seconds; the full forms are bench.py --form precision|batch|adjoint|slabs.
 
 def rel_l2(a, b):
     import numpy as np
@@ -954,6 +955,62 @@ SLAB_WORKLOADS = (
 )
 
 
+def slab_record(cfg: dict, counts, k, n: int, warm: int) -> dict:
+    """One slab workload: the whole grid by ifc_iterate, then the same solve
+    through ifc_slabs in 1 slab (the steps one stage at a time) and in each
+    count of overlapping slabs on this GPU, ms per outer iteration (host clock
+    around synchronised iterations: the slabs' steps are host-orchestrated),
+    with the halo traffic and a bit-for-bit check of u against the whole
+    grid's after the same iterations."""
+    import numpy as np
+    import torch
+
+    import ifc
+    import ifc_slabs as S
+
+    def timed(fn, reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(reps)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / reps
+
+    dim = cfg["dim"]
+    sweeps = cfg["nIter_u"] + cfg["nIter_v"] + (cfg["nIter_w"] if dim == 3 else 0) + cfg["nIter_p"]
+    cells = cfg["nx"] * cfg["ny"] * (cfg["nz"] if dim == 3 else 1)
+    whole_cfg = dict(cfg, tol_u=0.0, tol_v=0.0, tol_w=0.0, tol_p=0.0, tol_mass=0.0, pin_pressure=0)
+    s = ifc.Solver(whole_cfg)
+    s.iterate(warm)
+    ms_whole = timed(s.iterate, n)
+    ref_u = s.get("u")
+    s.close()
+    rec = {"cells": cells, "sweeps_per_outer": sweeps, "outer_iterations_timed": n,
+           "sweeps_per_exchange": k or "whole stages", "whole_ifc_iterate_ms_per_outer": ms_whole}
+    for parts in (1,) + tuple(counts):
+        with S.SlabSolver(cfg, parts=parts, sweeps_per_exchange=k) as ss:
+            ss.iterate(warm)
+            x0 = ss.exchanges
+            b0 = ss.halo.bytes if ss.halo is not None else 0
+            ms = timed(ss.iterate, n)
+            held = sum(g1 - g0 for g0, g1 in ss.plan.span)
+            rec["stages_1_slab" if parts == 1 else f"slabs_{parts}"] = {
+                "ms_per_outer": ms, "cell_updates_per_s": cells * sweeps / (ms * 1e-3),
+                "halo_rows": ss.plan.halo, "rows_held_over_rows": held / ss.plan.cells,
+                "exchanges_per_outer": (ss.exchanges - x0) / n,
+                "halo_bytes_per_outer": ((ss.halo.bytes if ss.halo is not None else 0) - b0) / n,
+                "bitwise_equal_to_whole": bool(np.array_equal(ss.gather("u"), ref_u))}
+    return rec
+
+
+def slabs_summary() -> dict:
+    """The compact slab record of the default line: the 4096 x 2048 channel,
+    whole and in 2 and 4 slabs, 3 outer iterations each."""
+    import ifc
+
+    name, make, counts, k, _ = SLAB_WORKLOADS[0]
+    return {"workload": name, **slab_record(make(ifc), counts, k, 3, 1)}
+
+
 def run_slabs(args):
     """Slab decomposition on one GPU (ifc_slabs): each workload's grid solved
     whole (ifc_iterate, and the same steps one stage at a time) and cut into
@@ -963,62 +1020,23 @@ def run_slabs(args):
     the cost of the decomposition itself, the part a multi-GPU run adds to
     each GPU's share of the work.  Each decomposed solve is checked bit for
     bit against the whole grid's after the same iterations."""
-    import numpy as np
     import torch
 
     import ifc
-    import ifc_slabs as S
 
     world, rank, local = dist_env()
     if rank != 0:
         return
     torch.cuda.set_device(local)
-    records = {}
     clocks = ClockSampler(local)
     clocks.start()
-
-    def timed(fn, n):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        fn(n)
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t0) * 1e3 / n
-
-    for name, make, counts, k, n in SLAB_WORKLOADS:
-        cfg = make(ifc)
-        dim = cfg["dim"]
-        sweeps = cfg["nIter_u"] + cfg["nIter_v"] + (cfg["nIter_w"] if dim == 3 else 0) + cfg["nIter_p"]
-        cells = cfg["nx"] * cfg["ny"] * (cfg["nz"] if dim == 3 else 1)
-        warm = max(args.warmup, 1)
-        whole_cfg = dict(cfg, tol_u=0.0, tol_v=0.0, tol_w=0.0, tol_p=0.0, tol_mass=0.0, pin_pressure=0)
-        s = ifc.Solver(whole_cfg)
-        s.iterate(warm)
-        ms_whole = timed(s.iterate, n)
-        ref_u = s.get("u")
-        s.close()
-        rec = {"cells": cells, "sweeps_per_outer": sweeps, "outer_iterations_timed": n,
-               "sweeps_per_exchange": k or "whole stages",
-               "whole_ifc_iterate_ms_per_outer": ms_whole}
-        for parts in (1,) + tuple(counts):
-            with S.SlabSolver(cfg, parts=parts, sweeps_per_exchange=k) as ss:
-                ss.iterate(warm)
-                x0 = ss.exchanges
-                b0 = ss.halo.bytes if ss.halo is not None else 0
-                ms = timed(ss.iterate, n)
-                exact = bool(np.array_equal(ss.gather("u"), ref_u))
-                held = sum(g1 - g0 for g0, g1 in ss.plan.span)
-                key = "stages_1_slab" if parts == 1 else f"slabs_{parts}"
-                rec[key] = {"ms_per_outer": ms, "cell_updates_per_s": cells * sweeps / (ms * 1e-3),
-                            "halo_rows": ss.plan.halo, "rows_held_over_rows": held / ss.plan.cells,
-                            "exchanges_per_outer": (ss.exchanges - x0) / n,
-                            "halo_bytes_per_outer": ((ss.halo.bytes if ss.halo is not None else 0) - b0) / n,
-                            "bitwise_equal_to_whole": exact}
-        records[name] = rec
+    records = {name: slab_record(make(ifc), counts, k, n, max(args.warmup, 1))
+               for name, make, counts, k, n in SLAB_WORKLOADS}
     clk = clocks.stop()
     base = records[SLAB_WORKLOADS[0][0]]
     line = {
         "metric": METRIC, "value": base["slabs_4"]["cell_updates_per_s"], "unit": METRIC, "n_gpus": 1,
-        "steps": n, "warmup": args.warmup, "ms_per_step": base["slabs_4"]["ms_per_outer"],
+        "steps": SLAB_WORKLOADS[0][4], "warmup": args.warmup, "ms_per_step": base["slabs_4"]["ms_per_outer"],
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: flows from rest",
         "config": {"workload": "slabs: " + ", ".join(w[0] for w in SLAB_WORKLOADS),

@@ -319,7 +319,10 @@ int ifc_run_stage(ifc_solver *h, int stage);
 
 /* n sweeps of one equation (0=u 1=v 2=w 3=p') with the coefficients and
  * sources currently materialised by IFC_STAGE_MOM_ASSEMBLE / PCORR_COEF;
- * sq_norms (optional, n entries) receives sum (d phi)^2 of each sweep. */
+ * sq_norms (optional, n entries) receives sum (d phi)^2 of each sweep.  With
+ * sq_norms NULL the n Gauss-Seidel sweeps run as one cooperative launch on
+ * the stored planes where the handle has one (2D; 3D when its p' solve is
+ * cooperative), else back to back, and the call waits for the device once. */
 int ifc_sweep(ifc_solver *h, int eq, int n, double *sq_norms);
 
 /* Average device time (ms, CUDA events on the handle's stream) of one launch

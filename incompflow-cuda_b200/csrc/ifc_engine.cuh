@@ -351,7 +351,15 @@ struct Engine : EngineBase {
         if (best < 0) return IFC_OK;
         const size_t smem = coop3d_smem_bytes<T>(b.bj * b.bk, nx);
         auto kern = k_csolve3d<T, kPcNT>;
-        IFC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // The limit is one setting of the kernel shared by every handle of
+        // the process, whose blocks need different amounts: set it to the
+        // device's maximum (less the kernel's static shared memory), so no
+        // handle lowers it below another's launch.
+        cudaFuncAttributes fa;
+        IFC_CK(cudaFuncGetAttributes(&fa, kern));
+        const int dyn_max = optin - (int)fa.sharedSizeBytes;
+        if ((long long)smem > dyn_max) return IFC_OK;
+        IFC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
         int per_sm = 0;
         IFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPcNT, smem));
         if (per_sm < 1 || (long long)per_sm * nsm < (long long)b.nbj * b.nbk) return IFC_OK;
@@ -876,14 +884,61 @@ struct Engine : EngineBase {
         T *src[1] = {eq == 0 ? f.su : eq == 1 ? f.sv : eq == 2 ? f.sw : f.sp};
         const int eqs[1] = {eq};
         const int one[1] = {1};
+        // Without sq: exactly n red-black sweeps on the stored planes as one
+        // cooperative launch where the handle has one (k_coef_solve2d in 2D,
+        // k_csolve3d in 3D; the same point updates in the same colour order,
+        // tolerance 0 so no early exit), and the host waits once.
+        if (!sq && n > 0 && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+            Params<T> PT = P;
+            PT.g.tol[eq] = 0.0;
+            const T *coef = eq == 3 ? f.pcoef : f.mc;
+            using S = TileShape2D<T>;
+            using R = Region<S::TX, S::TY, 10>;
+            const int tiles = ((P.g.nx + S::TX - 1) / S::TX) * ((P.g.ny + S::TY - 1) / S::TY);
+            const bool c2 = dim == 2 && fused && energy_coop(tiles);
+            const bool c3 = dim == 3 && pc3d;
+            if (c2 || c3) {
+                IFC_CK(cudaMemsetAsync(&ctl->status, 0, sizeof(int), stream));
+                k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << eq);
+                if (c3) {
+                    CSys<T> sys = {coef, src[0], phi[0], eq};
+                    enq_csolve3d(PT, sys, n);
+                } else {
+                    IFC_CK(cudaMemsetAsync(barrier, 0, sizeof(GridBarrier), stream));
+                    int e = eq, ns = n, stall = 0;
+                    T *x0 = phi[0], *x1 = f.tmp + 2 * (size_t)P.g.N;
+                    const T *srcp = src[0];
+                    void *args[] = {&PT, &coef, &srcp, &ctl, &partials, &barrier, &e, &ns, &x0, &x1, &stall};
+                    IFC_CK(cudaLaunchCooperativeKernel((const void *)k_coef_solve2d<T, S::TX, S::TY, 5, S::NT>,
+                                                       dim3(tiles), dim3(S::NT), args, R::NR * sizeof(T), stream));
+                    ++launches;
+                }
+                IFC_CK(cudaGetLastError());
+                int rc = read_ctl();
+                if (rc != IFC_OK) return rc;
+                if (ctl_h.status == 3) {
+                    err = "sweep: a grid barrier of the cooperative sweeps timed out";
+                    return IFC_TIMEOUT;
+                }
+                return bounds_status();
+            }
+        }
+        // With sq the host reads each sweep's sum; without it the n sweeps
+        // run back to back and the host waits once.
         for (int s = 0; s < n; ++s) {
             k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << eq);
             if (dim == 2) enq_sweeps<2, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
             else enq_sweeps<3, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
             IFC_CK(cudaGetLastError());
+            if (sq) {
+                int rc = read_ctl();
+                if (rc != IFC_OK) return rc;
+                sq[s] = ctl_h.last_sweep_sq[eq];
+            }
+        }
+        if (!sq) {
             int rc = read_ctl();
             if (rc != IFC_OK) return rc;
-            if (sq) sq[s] = ctl_h.last_sweep_sq[eq];
         }
         return bounds_status();
     }

@@ -341,7 +341,12 @@ class Solver:
     def stage(self, name: str):
         self._check(load().ifc_run_stage(self._h, STAGES.index(name)), f"stage {name}")
 
-    def sweep(self, eq: int, n: int = 1) -> np.ndarray:
+    def sweep(self, eq: int, n: int = 1, norms: bool = True) -> np.ndarray | None:
+        """n sweeps of equation eq; with norms, sum (d phi)^2 of each sweep
+        (the host then waits for every sweep; without, once at the end)."""
+        if not norms:
+            self._check(load().ifc_sweep(self._h, eq, n, None), "sweep")
+            return None
         sq = (C.c_double * max(n, 1))()
         self._check(load().ifc_sweep(self._h, eq, n, sq), "sweep")
         return np.array(sq[:n])

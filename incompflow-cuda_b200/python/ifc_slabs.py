@@ -187,7 +187,7 @@ class DeviceSlab:
         self.solver.stage(name)
 
     def sweep(self, eq: int, n: int):
-        self.solver.sweep(eq, n)
+        self.solver.sweep(eq, n, norms=False)
 
     def view(self, name: str) -> torch.Tensor:
         v = self._views.get(name)

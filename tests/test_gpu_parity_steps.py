@@ -133,3 +133,40 @@ def test_outer_iterations(gpu_ok, name, prec):
                 assert_bitwise(s.get(k), o.field(k), f"{name} it{it} {k}")
         for a, b in (("norm_u", "u"), ("norm_v", "v"), ("norm_p", "p"), ("norm_mass", "mass")):
             np.testing.assert_allclose(st[a], nm[b], rtol=1e-6, atol=1e-300)
+
+
+def _coop_cases():
+    c = dict(CASES)
+    c["channel96x40"] = dict(ifc.channel2d(96, 40), nIter_u=3, nIter_v=3, nIter_p=7)
+    c["cavity12x10x14"] = dict(ifc.cavity3d(12, nx=12, ny=10, nz=14), nIter_u=3, nIter_v=3, nIter_w=3, nIter_p=7)
+    return c
+
+
+COOP = _coop_cases()
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+@pytest.mark.parametrize("name", list(COOP))
+def test_sweeps_without_norms_bitwise(gpu_ok, name, prec):
+    """ifc_sweep without per-sweep norms runs the n sweeps as one cooperative
+    launch on the stored planes (k_coef_solve2d in 2D, k_csolve3d in 3D):
+    the fields must equal the oracle's n red-black sweeps bit for bit, for
+    every momentum component and p', from a seeded state."""
+    cfg = dict(COOP[name], precision=prec)
+    o = O.Oracle(to_oracle_cfg(cfg), prec)
+    s = ifc.Solver(cfg)
+    load_both(o, s, seeded_state(cfg, 13, s.dtype))
+    d3 = cfg["dim"] == 3
+    s.stage("face_bc"); o.init_face_vel(); o.bc_face_vel()
+    s.stage("mom_assemble"); o.mom_link_coef(); o.mom_src(); o.bc_mom()
+    for eq, k in enumerate(["u", "v"] + (["w"] if d3 else [])):
+        assert s.sweep(eq, 4, norms=False) is None
+        for _ in range(4):
+            o.sweep(eq, O.GS_REDBLACK)
+        assert_bitwise(s.get(k), o.field(k), f"{name} {k} after 4 sweeps")
+    s.stage("rhie_chow"); o.rhie_chow(); o.bc_face_vel(); o.pcorr_src()
+    s.stage("pcorr_coef"); o.pcorr_link_coef()
+    s.sweep(O.EQ_P, 6, norms=False)
+    for _ in range(6):
+        o.sweep(O.EQ_P, O.GS_REDBLACK)
+    assert_bitwise(s.get("pc"), o.field("pc"), f"{name} pc after 6 sweeps")

@@ -73,3 +73,16 @@ def test_slabs_match_oracle_3d(gpu_ok):
     o.bc_face_vel()
     for n in got:
         assert_bitwise(got[n], o.field(n), f"3d slabs vs oracle {n}")
+
+
+def test_3d_handles_of_different_sizes_coexist(gpu_ok):
+    """The cooperative 3D p' kernel's shared-memory limit is one setting
+    shared by every handle: a smaller handle created later must not break
+    the larger one's launches (as the slabs of one grid are)."""
+    a = ifc.Solver(ifc.cavity3d(16, nx=16, ny=16, nz=40))
+    b = ifc.Solver(ifc.cavity3d(8))
+    for s in (a, b, a):
+        st = s.iterate(2)
+        assert st["status"] == ifc.OK, st
+    a.close()
+    b.close()
