@@ -332,7 +332,7 @@ struct Engine : EngineBase {
         IFC_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         if (!coop) return IFC_OK;
         const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
-        const size_t per_row = sizeof(T) * (size_t)nx + 20;  // p' and the row table
+        const size_t per_row = sizeof(T) * (size_t)(2 * ((nx + 1) / 2)) + 20;  // p' and the row table
         const long long max_rows = ((long long)optin - 4096) / (long long)per_row;
         if (max_rows < 1) return IFC_OK;
         long long best = -1, best_per = 0;
