@@ -31,34 +31,6 @@
 
 namespace ifc {
 
-// Four consecutive values from a 16-byte aligned address, bypassing L1 (each
-// packed value is read once per half sweep).
-__device__ __forceinline__ void ld4(const float *p, float (&o)[4])
-{
-    const float4 v = __ldcg(reinterpret_cast<const float4 *>(p));
-    o[0] = v.x;
-    o[1] = v.y;
-    o[2] = v.z;
-    o[3] = v.w;
-}
-__device__ __forceinline__ void ld4(const double *p, double (&o)[4])
-{
-    const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
-    const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
-    o[0] = a.x;
-    o[1] = a.y;
-    o[2] = b.x;
-    o[3] = b.y;
-}
-template <typename T>
-__device__ __forceinline__ void st4(T *p, T a, T b, T c, T d)
-{
-    p[0] = a;
-    p[1] = b;
-    p[2] = c;
-    p[3] = d;
-}
-
 // Packed slots: per CTA rows_cap rows x 2 colours x hx cells, hx = (nx+1)/2;
 // the cell (i, row r, colour c) sits in slot (2r + c) * hx + (i >> 1) of its
 // CTA's range.  Two planes of 4 values per slot follow each other, each

@@ -144,6 +144,10 @@ struct Engine : EngineBase {
     PcBlocks pcb = {0, 0, 0, 0};
     size_t pc3d_smem = 0;
     T *packed = nullptr;
+    // The 3D momentum coefficients and sources of one solve, packed by the
+    // first sweep (k_mom_half3d<T, true>): 10 values per slot
+    T *mpk = nullptr;
+    long long mpk_slots = 0;
 
     ~Engine() override
     {
@@ -269,6 +273,10 @@ struct Engine : EngineBase {
         A_(f.ac, N); A_(f.mc, N * nc); A_(f.pcoef, N * nc);
         A_(f.su, N); A_(f.sv, N); A_(f.sw, N); A_(f.sp, N); A_(f.tmp, 3 * N); A_(f.rac, N);
         if (c.convection_scheme != IFC_CONV_UPWIND) A_(f.sdc, (size_t)dim * N);
+        if (dim == 3 && c.linear_solver == IFC_GAUSS_SEIDEL) {
+            mpk_slots = (long long)P.g.ny * P.g.nz * 2 * ((P.g.nx + 1) / 2);
+            A_(mpk, (size_t)mpk_slots * 10);
+        }
         // One FP64 partial per value and block: the grid-stride kernels use at
         // most max_grid blocks, the tiled 2D kernels one block per 32x8 tile.
         const size_t tiles = (size_t)((P.g.nx + 31) / 32) * (size_t)((P.g.ny + 7) / 8) * (size_t)P.g.nz;
@@ -561,7 +569,12 @@ struct Engine : EngineBase {
                 h.first = s == 0;
                 for (int color = 0; color < 2; ++color) {
                     h.color = color;
-                    k_mom_half3d<T><<<wave_grid((const void *)k_mom_half3d<T>, grid(half)), 256, 0, stream>>>(P, f, ctl, partials, h);
+                    if (s == 0)
+                        k_mom_half3d<T, true><<<wave_grid((const void *)k_mom_half3d<T, true>, grid(half)), 256, 0, stream>>>(
+                            P, f, ctl, partials, h, mpk, mpk_slots);
+                    else
+                        k_mom_half3d<T, false><<<wave_grid((const void *)k_mom_half3d<T, false>, grid(half)), 256, 0, stream>>>(
+                            P, f, ctl, partials, h, mpk, mpk_slots);
                     ++launches;
                 }
             }
