@@ -40,7 +40,17 @@ CASES = {
     # 5/5/5/50 sweeps: chunks of 4 (halo 12), or whole stages (halo 104)
     "cavity16x16x48_chunk4_3": (lambda: ifc.cavity3d(16, nx=16, ny=16, nz=48), 3, 4, 5),
     "cavity12x12x240_stages_2": (lambda: ifc.cavity3d(12, nx=12, ny=12, nz=240), 2, None, 3),
+    # higher-order convection, an inlet on a cut face and a west inlet profile
+    "mixed_quick96x72_chunk2_3": (lambda: _mixed_quick(), 3, 2, 6),
 }
+
+
+def _mixed_quick():
+    c = ifc.channel2d(96, 72, nIter_u=4, nIter_v=4, nIter_p=8, convection_scheme="quick")
+    c["velBC_type"] = [ifc.OUTLET, ifc.INLET, ifc.INLET, ifc.WALL, ifc.WALL, ifc.WALL]
+    c["velBC_val"] = [[0, 0, 0], [0.002, 0.0005, 0], [0.0003, -0.001, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]]
+    c["inlet_profile"] = np.linspace(0.0005, 0.0015, 72)
+    return c
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
