@@ -7,7 +7,7 @@ temporally blocked variants).  Every variant is run forced
 (IFC_BATCH_VARIANT) and as chosen by the autotuner.  Tolerance: relative L2
 1e-6 against the oracle with the same ordering (FP64 norms summed in a
 different order can move a convergence decision by one iteration), and the
-north star's 1e-4 against the FP64 lexicographic oracle."""
+converged-solution bound of 1e-4 against the FP64 lexicographic oracle."""
 import numpy as np
 import pytest
 

@@ -1,6 +1,6 @@
 """Converged solves on the GPU against the CPU oracle.
 
-Tolerances: the north star's relative L2 <= 1e-4 on converged u, v, w, p
+Tolerances: relative L2 <= 1e-4 on converged u, v, w, p
 (p after removing its mean in closed domains, where it is defined only up to a
 constant).  Against the oracle running the same red-black ordering the device
 must agree far tighter (1e-6), and usually bit for bit.
@@ -45,7 +45,7 @@ def test_converged_solve(gpu_ok, name):
     for k in dev:
         assert rel_l2(dev[k], same[k]) < 1e-6, (k, rel_l2(dev[k], same[k]))
 
-    # FP64, lexicographic oracle: the north-star tolerance.
+    # FP64, lexicographic oracle: the converged-solution tolerance 1e-4.
     o64 = O.Oracle(to_oracle_cfg(dict(cfg, sweep_mode=O.GS_LEX)), "d")
     o64.solve()
     ref = _fields(o64, lambda k: o64.field(k).copy(), cfg["dim"], closed)
@@ -111,7 +111,7 @@ def test_device_matches_reference_build(gpu_ok, name, closed, bound):
     tests/golden/, produced by its Solver::solve() on a B200): the same outer
     iterations from rest (3000; 10000 for the 512 x 128 bench channel, in one
     solve() call); bound 1e-5 relative L2, the resolution of the
-    reference's 6-digit VTK output being ~1e-6 (the north star asks 1e-4).
+    reference's 6-digit VTK output being ~1e-6 (converged solutions are held to 1e-4).
     On the 512 x 128 channel both FP32 solutions sit at the FP32 round-off
     floor of the pressure, 1.2e-5 apart (each 5e-5 from the FP64 answer), so
     that case is held to 3e-5."""
