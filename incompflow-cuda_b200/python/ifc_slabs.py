@@ -356,6 +356,7 @@ class SlabSolver:
         self.iterations = 0
         self.exchanges = 0
         self._faces_set = False
+        self._peak_mass = 0.0
 
     def _on_stream(self):
         return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
@@ -414,6 +415,24 @@ class SlabSolver:
         return {"outer_iterations": self.iterations, "exchanges": self.exchanges,
                 "halo_bytes": self.halo.bytes if self.halo is not None else 0,
                 "norm_mass": self.norm_mass() if self.iterations else 0.0}
+
+    def solve(self, tol_mass: float = 1e-5, max_outer: int | None = None, check_every: int = 50) -> dict:
+        """Outer iterations in blocks of check_every until the whole grid's
+        mass imbalance falls below tol_mass times its largest value at the
+        checks so far (the slab form's stopping rule: the reference's
+        per-field rules need correction norms of every field over the whole
+        grid), or until the handle has run max_outer outer iterations in all
+        (default: the config's numOuterIter)."""
+        limit = int(self.cfg["numOuterIter"] if max_outer is None else max_outer)
+        st = {"outer_iterations": self.iterations, "converged": False}
+        while self.iterations < limit:
+            st = self.iterate(min(check_every, limit - self.iterations))
+            self._peak_mass = max(self._peak_mass, st["norm_mass"])
+            st["rel_mass"] = st["norm_mass"] / self._peak_mass if self._peak_mass > 0 else 0.0
+            st["converged"] = st["rel_mass"] < tol_mass
+            if st["converged"]:
+                break
+        return st
 
     # ---- whole-grid views
     def _owned(self, s: int, name: str) -> torch.Tensor:

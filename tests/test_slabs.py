@@ -174,3 +174,18 @@ def test_two_gloo_ranks_bitwise(name):
     cfg = make()
     ref = undecomposed(cfg, its, "f")
     assert_equal_fields(got, {n: ref.field(n) for n in state_names(cfg["dim"])}, f"gloo {name}")
+
+
+def test_solve_stops_on_the_whole_grid_mass_imbalance():
+    """solve() runs blocks of outer iterations until the mass imbalance over
+    the whole grid (formed from the slabs' owned rows) falls below tol_mass
+    times its largest value at the checks; the fields are still bit for bit
+    those of the undecomposed oracle after the same number of iterations."""
+    cfg = ifc.cavity2d(16, ny=48, nIter_u=3, nIter_v=3, nIter_p=8)
+    ss = S.SlabSolver(cfg, parts=2, make_slab=_oracle_factory("d"))
+    st = ss.solve(tol_mass=0.15, max_outer=400, check_every=25)
+    assert st["converged"] and st["rel_mass"] < 0.15, st
+    assert st["outer_iterations"] % 25 == 0 and st["outer_iterations"] < 400
+    _compare(ss, cfg, st["outer_iterations"], "d", "solve")
+    st2 = ss.solve(tol_mass=0.0, max_outer=st["outer_iterations"] + 5, check_every=25)
+    assert st2["outer_iterations"] == st["outer_iterations"] + 5 and not st2["converged"]
