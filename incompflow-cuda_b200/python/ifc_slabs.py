@@ -475,6 +475,20 @@ class SlabSolver:
                 mine.update(d)
         return np.concatenate([mine[s] for s in range(self.plan.parts)])
 
+    def write_vtk(self, path: str, binary: bool = False):
+        """The whole grid's VTK file (ASCII RECTILINEAR_GRID as
+        Solver::writeVTK writes it, src/Solver.cu:301-367, or binary=True for
+        legacy VTK BINARY) from the gathered fields, byte for byte the file an
+        undecomposed handle writes; in the distributed form rank 0 writes it
+        (every rank takes part in the gathers)."""
+        f = {n: self.gather(n) for n in ("u", "v", "w", "p", "T")}
+        if self.group is not None:
+            import torch.distributed as dist
+
+            if dist.get_rank(self.group) != 0:
+                return
+        ifc.write_vtk_host(self.cfg, f["u"], f["v"], f["w"], f["p"], f["T"], path, binary)
+
     def load(self, name: str, values):
         """Set a field of the whole grid (reference layout) on every slab."""
         a = torch.as_tensor(np.ascontiguousarray(values).ravel())

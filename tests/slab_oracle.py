@@ -65,6 +65,8 @@ class OracleSlab:
         if v is None:
             if name == "ac":
                 a = self.o.field("mcoef")[: self.N]
+            elif name == "T":  # the oracle has no temperature: the handles' initial 273 K
+                a = np.full(self.N, 273.0, dtype=self.o.field("u").dtype)
             else:
                 a = self.o.field(name)
             v = torch.from_numpy(a)

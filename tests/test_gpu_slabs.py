@@ -96,3 +96,20 @@ def test_3d_handles_of_different_sizes_coexist(gpu_ok):
         assert st["status"] == ifc.OK, st
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name", ["channel128x96_stages_2", "cavity16x16x48_chunk4_3"])
+def test_slab_vtk_equals_the_whole_handle_file(gpu_ok, tmp_path, name):
+    """The VTK file written from the slabs' gathered fields is byte for byte
+    the file the undecomposed handle writes after the same iterations."""
+    make, parts, k, its = CASES[name]
+    cfg = make()
+    whole, _ = _undecomposed(cfg, its)
+    a = tmp_path / "whole.vtk"
+    whole.write_vtk(str(a))
+    whole.close()
+    with S.SlabSolver(cfg, parts=parts, sweeps_per_exchange=k) as ss:
+        ss.iterate(its)
+        b = tmp_path / "slabs.vtk"
+        ss.write_vtk(str(b))
+    assert a.read_bytes() == b.read_bytes()

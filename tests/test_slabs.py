@@ -189,3 +189,20 @@ def test_solve_stops_on_the_whole_grid_mass_imbalance():
     _compare(ss, cfg, st["outer_iterations"], "d", "solve")
     st2 = ss.solve(tol_mass=0.0, max_outer=st["outer_iterations"] + 5, check_every=25)
     assert st2["outer_iterations"] == st["outer_iterations"] + 5 and not st2["converged"]
+
+
+@pytest.mark.parametrize("binary", [False, True])
+def test_write_vtk_equals_the_whole_grid_file(tmp_path, binary):
+    """The VTK file from the slabs' gathered fields is byte for byte the one
+    the writer makes from the undecomposed oracle's fields."""
+    make, parts, k, its = CASES["cavity6x5x30_chunk1_3"]
+    cfg = make()
+    ss = S.SlabSolver(cfg, parts=parts, sweeps_per_exchange=k, make_slab=_oracle_factory("f"))
+    ss.iterate(its)
+    a = tmp_path / "slabs.vtk"
+    ss.write_vtk(str(a), binary=binary)
+    ref = undecomposed(cfg, its, "f")
+    b = tmp_path / "whole.vtk"
+    T = np.full(ref.field("u").size, 273.0, dtype=np.float32)
+    ifc.write_vtk_host(cfg, ref.field("u"), ref.field("v"), ref.field("w"), ref.field("p"), T, str(b), binary)
+    assert a.read_bytes() == b.read_bytes()
