@@ -57,8 +57,9 @@ class OracleSlab:
         self.first = False
 
     def sweep(self, eq: int, n: int):
+        mode = self.o.cfg["sweep_mode"]  # red-black Gauss-Seidel or Jacobi, as the config says
         for _ in range(n):
-            self.o.sweep(eq, O.GS_REDBLACK)
+            self.o.sweep(eq, mode)
 
     def view(self, name: str) -> torch.Tensor:
         v = self._views.get(name)

@@ -40,6 +40,8 @@ CASES = {
     # 5/5/5/50 sweeps: chunks of 4 (halo 12), or whole stages (halo 104)
     "cavity16x16x48_chunk4_3": (lambda: ifc.cavity3d(16, nx=16, ny=16, nz=48), 3, 4, 5),
     "cavity12x12x240_stages_2": (lambda: ifc.cavity3d(12, nx=12, ny=12, nz=240), 2, None, 3),
+    # Jacobi sweeps, whole stages between exchanges
+    "channel128x96_jacobi_stages_2": (lambda: ifc.channel2d(128, 96, linear_solver=ifc.JACOBI), 2, None, 8),
     # higher-order convection, an inlet on a cut face and a west inlet profile
     "mixed_quick96x72_chunk2_3": (lambda: _mixed_quick(), 3, 2, 6),
 }

@@ -104,6 +104,10 @@ CASES = {
                                                    nIter_p=4), 3, 1, 3),
     "cavity6x5x30_stages_2": (lambda: ifc.cavity3d(6, nx=6, ny=5, nz=30, nIter_u=2, nIter_v=2, nIter_w=2,
                                                    nIter_p=4), 2, None, 3),
+    "channel24x60_jacobi_chunk2_3": (lambda: ifc.channel2d(24, 60, nIter_u=3, nIter_v=3, nIter_p=5,
+                                                           linear_solver=ifc.JACOBI), 3, 2, 4),
+    "channel24x60_jacobi_stages_2": (lambda: ifc.channel2d(24, 60, nIter_u=3, nIter_v=3, nIter_p=5,
+                                                           linear_solver=ifc.JACOBI), 2, None, 4),
 }
 
 
@@ -157,19 +161,22 @@ def _gloo_worker(rank, world, port, q, name, prec):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name", ["channel24x40_stages_2", "cavity6x5x30_chunk1_3"])
-def test_two_gloo_ranks_bitwise(name):
+@pytest.mark.parametrize("name,world", [("channel24x40_stages_2", 2), ("cavity6x5x30_chunk1_3", 2),
+                                        ("cavity6x5x30_chunk1_3", 3)])
+def test_gloo_ranks_bitwise(name, world):
+    """One slab per gloo rank; with three ranks the middle one swaps halos
+    with both neighbours in one grouped exchange."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 29700 + (os.getpid() + len(name)) % 1000
-    procs = [ctx.Process(target=_gloo_worker, args=(r, 2, port, q, name, "f")) for r in range(2)]
+    port = 29700 + (os.getpid() + len(name) + 7 * world) % 1000
+    procs = [ctx.Process(target=_gloo_worker, args=(r, world, port, q, name, "f")) for r in range(world)]
     for p in procs:
         p.start()
     st, got, plan = q.get(timeout=120)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert plan.parts == 2 and st["exchanges"] > 0
+    assert plan.parts == world and st["exchanges"] > 0
     make, _, _, its = CASES[name]
     cfg = make()
     ref = undecomposed(cfg, its, "f")
