@@ -1025,7 +1025,8 @@ def run_slabs(args):
     import ifc
 
     world, rank, local = dist_env()
-    if rank != 0:
+    if world > 1:
+        run_slabs_ranks(args, world, rank, local)
         return
     torch.cuda.set_device(local)
     clocks = ClockSampler(local)
@@ -1046,6 +1047,72 @@ def run_slabs(args):
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
+
+
+def run_slabs_ranks(args, world: int, rank: int, local: int):
+    """Slab form on N GPUs (torchrun, one process per GPU): each workload's
+    grid cut into N slabs, one per rank, halos swapped with the two neighbour
+    ranks by NCCL send/receive after every step (ifc_slabs.DistHalo).  Time
+    per outer iteration is the max over ranks of host-clock time around
+    synchronised iterations (barrier on both sides); strong scaling (the grid
+    is fixed).  Rank 0 then checks u bit for bit against the whole grid solved
+    on its own GPU."""
+    from datetime import timedelta
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import ifc
+    import ifc_slabs as S
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    records = {}
+    for name, make, _, k, n in SLAB_WORKLOADS:
+        cfg = make(ifc)
+        dim = cfg["dim"]
+        sweeps = cfg["nIter_u"] + cfg["nIter_v"] + (cfg["nIter_w"] if dim == 3 else 0) + cfg["nIter_p"]
+        cells = cfg["nx"] * cfg["ny"] * (cfg["nz"] if dim == 3 else 1)
+        ss = S.SlabSolver(cfg, sweeps_per_exchange=k, group=dist.group.WORLD)
+        warm = max(args.warmup, 1)
+        ss.iterate(warm)
+        x0, b0 = ss.exchanges, ss.halo.bytes
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        ss.iterate(n)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ms = torch.tensor([(time.perf_counter() - t0) * 1e3 / n], dtype=torch.float64, device="cuda")
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        u = ss.gather("u")
+        rec = {"cells": cells, "slabs": world, "halo_rows": ss.plan.halo,
+               "sweeps_per_exchange": k or "whole stages", "ms_per_outer": float(ms[0]),
+               "cell_updates_per_s": cells * sweeps / (float(ms[0]) * 1e-3),
+               "exchanges_per_outer": (ss.exchanges - x0) / n,
+               "halo_bytes_per_outer_this_rank": (ss.halo.bytes - b0) / n}
+        ss.close()
+        if rank == 0:
+            w = ifc.Solver(dict(cfg, tol_u=0.0, tol_v=0.0, tol_w=0.0, tol_p=0.0, tol_mass=0.0, pin_pressure=0))
+            w.iterate(warm + n)
+            rec["bitwise_equal_to_whole"] = bool(np.array_equal(u, w.get("u")))
+            w.close()
+        records[name] = rec
+        dist.barrier()
+    if rank == 0:
+        base = records[SLAB_WORKLOADS[0][0]]
+        print(json.dumps({
+            "metric": METRIC, "value": base["cell_updates_per_s"], "unit": METRIC, "n_gpus": world,
+            "steps": SLAB_WORKLOADS[0][4], "warmup": args.warmup, "ms_per_step": base["ms_per_outer"],
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: flows from rest",
+            "config": {"workload": "slabs: " + ", ".join(w[0] for w in SLAB_WORKLOADS),
+                       "headline_value": f"channel2d_4096x2048 in {world} slabs, one per GPU",
+                       "timing": "host clock around synchronised outer iterations, max over ranks"},
+            "records": records}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
 
 
 def run_convergence(args):
