@@ -317,6 +317,17 @@ enum {
 };
 int ifc_run_stage(ifc_solver *h, int stage);
 
+/* The same launches on the handle's stream without waiting for them (for a
+ * caller that orders its own work after them on that stream, such as halo
+ * copies or NCCL transfers between slabs); their outcome -- a bounded wait
+ * that ran out (IFC_TIMEOUT), an index out of range in the bounds-checked
+ * build -- is reported by the next ifc_sync. */
+int ifc_run_stage_async(ifc_solver *h, int stage);
+
+/* Wait for the handle's stream and report what its launches left in the
+ * control block (IFC_OK, IFC_TIMEOUT, IFC_BAD_ARGUMENT). */
+int ifc_sync(ifc_solver *h);
+
 /* n sweeps of one equation (0=u 1=v 2=w 3=p') with the coefficients and
  * sources currently materialised by IFC_STAGE_MOM_ASSEMBLE / PCORR_COEF;
  * sq_norms (optional, n entries) receives sum (d phi)^2 of each sweep.  With

@@ -31,6 +31,8 @@ struct EngineBase {
     virtual void *device_ptr(int field) = 0;
     virtual int run(int n_outer, int act, ifc_stats *st) = 0;
     virtual int run_stage(int stage) = 0;
+    virtual int run_stage_async(int stage) = 0;
+    virtual int sync() = 0;
     virtual int sweep(int eq, int n, double *sq) = 0;
     virtual int stats(ifc_stats *st) = 0;
     virtual int time_stage(int stage, int reps, double *ms, int *launches) = 0;
@@ -832,9 +834,39 @@ struct Engine : EngineBase {
         if (dim == 2) run_stage_t<2>(stage);
         else run_stage_t<3>(stage);
         IFC_CK(cudaGetLastError());
+        return sync();
+    }
+
+    // The stage's launches on the handle's stream, without waiting: a caller
+    // that orders its own work after them on the same stream (the slab halo
+    // copies, NCCL transfers) reads their outcome at the next sync().
+    int run_stage_async(int stage) override
+    {
+        if (stage < 0 || stage >= IFC_STAGE_COUNT) {
+            err = "unknown stage";
+            return IFC_BAD_ARGUMENT;
+        }
+        if (dim == 2) run_stage_t<2>(stage);
+        else run_stage_t<3>(stage);
+        IFC_CK(cudaGetLastError());
+        return IFC_OK;
+    }
+
+    // Wait for the handle's stream; report a bounded wait that ran out
+    // (control-block status 3) and, in the bounds-checked build, an index out
+    // of range.
+    int sync() override
+    {
         IFC_CK(cudaStreamSynchronize(stream));
         const int rc = read_ctl();
-        return rc != IFC_OK ? rc : bounds_status();
+        if (rc != IFC_OK) return rc;
+        if (ctl_h.status == 3) {  // reported once: cleared for the handle's next launches
+            IFC_CK(cudaMemsetAsync(&ctl->status, 0, sizeof(int), stream));
+            IFC_CK(cudaStreamSynchronize(stream));
+            err = "a grid barrier of a cooperative launch timed out";
+            return IFC_TIMEOUT;
+        }
+        return bounds_status();
     }
 
     template <int DIM>

@@ -227,6 +227,20 @@ int ifc_run_stage(ifc_solver *h, int stage)
     IFC_END(h)
 }
 
+int ifc_run_stage_async(ifc_solver *h, int stage)
+{
+    IFC_GUARD(h)
+    return h->eng->run_stage_async(stage);
+    IFC_END(h)
+}
+
+int ifc_sync(ifc_solver *h)
+{
+    IFC_GUARD(h)
+    return h->eng->sync();
+    IFC_END(h)
+}
+
 int ifc_sweep(ifc_solver *h, int eq, int n, double *sq_norms)
 {
     IFC_GUARD(h)

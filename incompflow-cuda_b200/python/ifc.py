@@ -126,6 +126,8 @@ EXPORTS = {
     "ifc_write_vtk_binary_host": (C.c_int, [C.POINTER(IfcConfig)] + [C.c_void_p] * 5 + [C.c_char_p]),
     "ifc_run_stage": (C.c_int, [C.c_void_p, C.c_int]),
     "ifc_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "ifc_run_stage_async": (C.c_int, [C.c_void_p, C.c_int]),
+    "ifc_sync": (C.c_int, [C.c_void_p]),
     "ifc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(IfcStats)]),
     "ifc_time_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "ifc_last_error": (C.c_char_p, [C.c_void_p]),
@@ -338,8 +340,16 @@ class Solver:
         self._check(load().ifc_iterate(self._h, int(n), C.byref(st)), "iterate")
         return st.as_dict()
 
-    def stage(self, name: str):
-        self._check(load().ifc_run_stage(self._h, STAGES.index(name)), f"stage {name}")
+    def stage(self, name: str, wait: bool = True):
+        """One step of the outer iteration; wait=False enqueues its launches
+        on the handle's stream and returns (outcome at the next sync())."""
+        fn = load().ifc_run_stage if wait else load().ifc_run_stage_async
+        self._check(fn(self._h, STAGES.index(name)), f"stage {name}")
+
+    def sync(self):
+        """Wait for the handle's stream; raises on a timed-out wait or an
+        out-of-range index left by enqueued launches."""
+        self._check(load().ifc_sync(self._h), "sync")
 
     def sweep(self, eq: int, n: int = 1, norms: bool = True) -> np.ndarray | None:
         """n sweeps of equation eq; with norms, sum (d phi)^2 of each sweep

@@ -184,7 +184,12 @@ class DeviceSlab:
         self._views = {}
 
     def stage(self, name: str):
-        self.solver.stage(name)
+        # enqueued only: the halo copies or NCCL transfers that follow on the
+        # same stream are ordered after it, and sync() reports its outcome
+        self.solver.stage(name, wait=False)
+
+    def sync(self):
+        self.solver.sync()
 
     def sweep(self, eq: int, n: int):
         self.solver.sweep(eq, n, norms=False)
@@ -412,6 +417,8 @@ class SlabSolver:
                 self._sweeps({3: int(c["nIter_p"])})
                 self._step("update")
             self.iterations += 1
+        for s in self.local:
+            self.slabs[s].sync()
         return {"outer_iterations": self.iterations, "exchanges": self.exchanges,
                 "halo_bytes": self.halo.bytes if self.halo is not None else 0,
                 "norm_mass": self.norm_mass() if self.iterations else 0.0}

@@ -74,6 +74,9 @@ class OracleSlab:
             self._views[name] = v
         return v
 
+    def sync(self):
+        pass
+
     def zero(self, name: str):
         self.view(name).zero_()
 
