@@ -324,6 +324,10 @@ int ifc_run_stage(ifc_solver *h, int stage);
  * build -- is reported by the next ifc_sync. */
 int ifc_run_stage_async(ifc_solver *h, int stage);
 
+/* ifc_sweep without norms (n sweeps as one cooperative launch where the
+ * handle has one), enqueued without waiting; outcome at the next ifc_sync. */
+int ifc_sweep_async(ifc_solver *h, int eq, int n);
+
 /* Wait for the handle's stream and report what its launches left in the
  * control block (IFC_OK, IFC_TIMEOUT, IFC_BAD_ARGUMENT). */
 int ifc_sync(ifc_solver *h);

@@ -34,6 +34,7 @@ struct EngineBase {
     virtual int run_stage_async(int stage) = 0;
     virtual int sync() = 0;
     virtual int sweep(int eq, int n, double *sq) = 0;
+    virtual int sweep_async(int eq, int n) = 0;
     virtual int stats(ifc_stats *st) = 0;
     virtual int time_stage(int stage, int reps, double *ms, int *launches) = 0;
     virtual int adjoint(const AdjointReq &rq, ifc_adjoint_result *res) = 0;
@@ -925,25 +926,54 @@ struct Engine : EngineBase {
             err = "sweep: bad equation or count";
             return IFC_BAD_ARGUMENT;
         }
+        if (!sq) {
+            const int rc = enq_sweeps_stored(eq, n);
+            return rc != IFC_OK ? rc : sync();
+        }
+        // With sq the host reads each sweep's sum.
         T *phi[1] = {eq == 0 ? f.u : eq == 1 ? f.v : eq == 2 ? f.w : f.pc};
         T *src[1] = {eq == 0 ? f.su : eq == 1 ? f.sv : eq == 2 ? f.sw : f.sp};
         const int eqs[1] = {eq};
         const int one[1] = {1};
-        // Without sq: exactly n red-black sweeps on the stored planes as one
-        // cooperative launch where the handle has one (k_coef_solve2d in 2D,
-        // k_csolve3d in 3D; the same point updates in the same colour order,
-        // tolerance 0 so no early exit), and the host waits once.
-        if (!sq && n > 0 && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
+        for (int s = 0; s < n; ++s) {
+            k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << eq);
+            if (dim == 2) enq_sweeps<2, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
+            else enq_sweeps<3, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
+            IFC_CK(cudaGetLastError());
+            int rc = read_ctl();
+            if (rc != IFC_OK) return rc;
+            sq[s] = ctl_h.last_sweep_sq[eq];
+        }
+        return bounds_status();
+    }
+
+    int sweep_async(int eq, int n) override
+    {
+        if (eq < 0 || eq > 3 || (eq == 2 && dim == 2) || n < 0) {
+            err = "sweep: bad equation or count";
+            return IFC_BAD_ARGUMENT;
+        }
+        return enq_sweeps_stored(eq, n);
+    }
+
+    // Exactly n red-black sweeps of equation eq on the stored planes, enqueued:
+    // one cooperative launch where the handle has one (k_coef_solve2d in 2D,
+    // k_csolve3d in 3D; the same point updates in the same colour order,
+    // tolerance 0 so no early exit), else a launch pair per sweep.
+    int enq_sweeps_stored(int eq, int n)
+    {
+        T *phi[1] = {eq == 0 ? f.u : eq == 1 ? f.v : eq == 2 ? f.w : f.pc};
+        T *src[1] = {eq == 0 ? f.su : eq == 1 ? f.sv : eq == 2 ? f.sw : f.sp};
+        const T *coef = eq == 3 ? f.pcoef : f.mc;
+        if (n > 0 && cfg.linear_solver == IFC_GAUSS_SEIDEL) {
             Params<T> PT = P;
             PT.g.tol[eq] = 0.0;
-            const T *coef = eq == 3 ? f.pcoef : f.mc;
             using S = TileShape2D<T>;
             using R = Region<S::TX, S::TY, 10>;
             const int tiles = ((P.g.nx + S::TX - 1) / S::TX) * ((P.g.ny + S::TY - 1) / S::TY);
             const bool c2 = dim == 2 && fused && energy_coop(tiles);
             const bool c3 = dim == 3 && pc3d;
             if (c2 || c3) {
-                IFC_CK(cudaMemsetAsync(&ctl->status, 0, sizeof(int), stream));
                 k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << eq);
                 if (c3) {
                     CSys<T> sys = {coef, src[0], phi[0], eq};
@@ -959,33 +989,18 @@ struct Engine : EngineBase {
                     ++launches;
                 }
                 IFC_CK(cudaGetLastError());
-                int rc = read_ctl();
-                if (rc != IFC_OK) return rc;
-                if (ctl_h.status == 3) {
-                    err = "sweep: a grid barrier of the cooperative sweeps timed out";
-                    return IFC_TIMEOUT;
-                }
-                return bounds_status();
+                return IFC_OK;
             }
         }
-        // With sq the host reads each sweep's sum; without it the n sweeps
-        // run back to back and the host waits once.
+        const int eqs[1] = {eq};
+        const int one[1] = {1};
         for (int s = 0; s < n; ++s) {
             k_reset_inner<<<1, 1, 0, stream>>>(ctl, 1 << eq);
-            if (dim == 2) enq_sweeps<2, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
-            else enq_sweeps<3, 1>(eq == 3 ? f.pcoef : f.mc, phi, src, eqs, one);
-            IFC_CK(cudaGetLastError());
-            if (sq) {
-                int rc = read_ctl();
-                if (rc != IFC_OK) return rc;
-                sq[s] = ctl_h.last_sweep_sq[eq];
-            }
+            if (dim == 2) enq_sweeps<2, 1>(coef, phi, src, eqs, one);
+            else enq_sweeps<3, 1>(coef, phi, src, eqs, one);
         }
-        if (!sq) {
-            int rc = read_ctl();
-            if (rc != IFC_OK) return rc;
-        }
-        return bounds_status();
+        IFC_CK(cudaGetLastError());
+        return IFC_OK;
     }
 
     // Steady temperature on the current flow (ifc_energy.cuh): assemble the

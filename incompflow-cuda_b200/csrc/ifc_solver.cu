@@ -234,6 +234,13 @@ int ifc_run_stage_async(ifc_solver *h, int stage)
     IFC_END(h)
 }
 
+int ifc_sweep_async(ifc_solver *h, int eq, int n)
+{
+    IFC_GUARD(h)
+    return h->eng->sweep_async(eq, n);
+    IFC_END(h)
+}
+
 int ifc_sync(ifc_solver *h)
 {
     IFC_GUARD(h)

@@ -127,6 +127,7 @@ EXPORTS = {
     "ifc_run_stage": (C.c_int, [C.c_void_p, C.c_int]),
     "ifc_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "ifc_run_stage_async": (C.c_int, [C.c_void_p, C.c_int]),
+    "ifc_sweep_async": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "ifc_sync": (C.c_int, [C.c_void_p]),
     "ifc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(IfcStats)]),
     "ifc_time_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
@@ -351,11 +352,16 @@ class Solver:
         out-of-range index left by enqueued launches."""
         self._check(load().ifc_sync(self._h), "sync")
 
-    def sweep(self, eq: int, n: int = 1, norms: bool = True) -> np.ndarray | None:
+    def sweep(self, eq: int, n: int = 1, norms: bool = True, wait: bool = True) -> np.ndarray | None:
         """n sweeps of equation eq; with norms, sum (d phi)^2 of each sweep
-        (the host then waits for every sweep; without, once at the end)."""
+        (the host then waits for every sweep); without, one cooperative
+        launch where the handle has one, waited for once, or with wait=False
+        only enqueued (outcome at the next sync())."""
         if not norms:
-            self._check(load().ifc_sweep(self._h, eq, n, None), "sweep")
+            if wait:
+                self._check(load().ifc_sweep(self._h, eq, n, None), "sweep")
+            else:
+                self._check(load().ifc_sweep_async(self._h, eq, n), "sweep_async")
             return None
         sq = (C.c_double * max(n, 1))()
         self._check(load().ifc_sweep(self._h, eq, n, sq), "sweep")

@@ -192,7 +192,7 @@ class DeviceSlab:
         self.solver.sync()
 
     def sweep(self, eq: int, n: int):
-        self.solver.sweep(eq, n, norms=False)
+        self.solver.sweep(eq, n, norms=False, wait=False)
 
     def view(self, name: str) -> torch.Tensor:
         v = self._views.get(name)
