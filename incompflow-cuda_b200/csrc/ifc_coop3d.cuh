@@ -64,7 +64,8 @@ struct CSys {
 
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 1) k_csolve3d(Params<T> P, Fields<T> f, Ctl *ctl, double *partials,
-                                                    GridBarrier *bar, PcBlocks B, int n_sweeps, T *pk, CSys<T> sys)
+                                                    GridBarrier *bar, PcBlocks B, int n_sweeps, T *pk, CSys<T> sys,
+                                                    int stall_test)
 {
     const Geo<T> &g = P.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, pl = nx * ny, N = g.N;
@@ -135,7 +136,10 @@ __global__ void __launch_bounds__(NT, 1) k_csolve3d(Params<T> P, Fields<T> f, Ct
     unsigned int epoch = 0;
     __syncthreads();  // the packed values are read back by the same CTA only
 
-    bool failed = false;
+    // Failure-detection test (IFC_TEST_STALL_BARRIER=1): CTA 0 leaves before
+    // its first grid barrier, so every other CTA's bounded wait runs out and
+    // the launch ends with the timeout status.
+    bool failed = stall_test && blockIdx.x == 0;
     for (int s = 0; s < n_sweeps && !stop && !failed; ++s) {
         for (int color = 0; color < 2; ++color) {
             const int zero_mode = (zero_start && s == 0) ? (color == 0 ? 1 : 2) : 0;

@@ -397,7 +397,9 @@ struct Engine : EngineBase {
         at[0].val.cooperative = 1;
         lc.attrs = at;
         lc.numAttrs = 1;
-        cudaLaunchKernelEx(&lc, k_csolve3d<T, kPcNT>, PP, f, ctl, partials, barrier, pcb, n, packed, sys);
+        const char *stall_env = std::getenv("IFC_TEST_STALL_BARRIER");  // failure-detection test, per launch
+        const int stall = (stall_env && stall_env[0] == '1') ? 1 : 0;
+        cudaLaunchKernelEx(&lc, k_csolve3d<T, kPcNT>, PP, f, ctl, partials, barrier, pcb, n, packed, sys, stall);
         ++launches;
     }
 

@@ -62,3 +62,24 @@ def test_energy_barrier_timeout_is_reported_and_handle_stays_usable(gpu_ok, monk
     assert np.isfinite(s.get("T")).all()
     st = s.iterate(3)
     assert st["status"] == ifc.OK
+
+
+def test_3d_cooperative_timeout_is_reported_at_sync_and_handle_stays_usable(gpu_ok, monkeypatch):
+    """The cooperative 3D p' solve (k_csolve3d) enqueued without a host wait,
+    with CTA 0 leaving before its first grid barrier: the other CTAs' bounded
+    waits run out, ifc_sync reports TIMEOUT, and the same handle then runs
+    the stage and whole outer iterations normally."""
+    s = ifc.Solver(ifc.cavity3d(16))
+    s.iterate(5)
+    s.stage("mom_solve")
+    s.stage("rhie_chow")
+    monkeypatch.setenv("IFC_TEST_STALL_BARRIER", "1")
+    s.stage("pcorr_solve", wait=False)
+    with pytest.raises(ifc.IfcError) as e:
+        s.sync()
+    assert e.value.status == ifc.TIMEOUT
+    monkeypatch.delenv("IFC_TEST_STALL_BARRIER")
+    s.stage("pcorr_solve")
+    st = s.iterate(3)
+    assert st["status"] == ifc.OK and st["outer_iterations"] == 8
+    assert np.isfinite(s.get("u")).all()
