@@ -38,7 +38,12 @@ Two exchanges: ``LocalHalo`` for slabs held by one process (device copies on
 one stream), ``DistHalo`` for one slab per rank of a ``torch.distributed``
 group (NCCL point-to-point over NVLink between GPUs; gloo for CPU tensors).
 Slabs are created by a factory, by default ``DeviceSlab`` (an ``ifc.Solver``
-with torch views of its device fields).
+with torch views of its device fields).  Device slabs enqueue their steps
+without a host wait (``ifc_run_stage_async``, ``ifc_sweep_async``), so steps,
+halo copies and NCCL transfers follow one another on one stream and the host
+waits once per ``iterate`` call.  ``solve`` stops on the whole grid's mass
+imbalance; ``gather`` and ``write_vtk`` give the whole grid's fields and VTK
+file, byte for byte those of an undecomposed handle.
 """
 from __future__ import annotations
 
