@@ -205,6 +205,30 @@ def cpu_baseline(seconds: float):
                       f"gcc -O2), {dt:.1f} s on one core of {host_cpu()}"}
 
 
+def cpu_baseline_all_cores(seconds: float):
+    """The same restatement built with OpenMP row loops
+    (oracle/_build/libifc_oracle_omp.so) on every host core, timed by
+    oracle/time_port.py in a child process (the parallel build's FP64 sweep
+    sums add in another order; each cell is computed as in the serial
+    build).  A separate record beside the one-core baseline."""
+    import subprocess
+
+    threads = os.cpu_count() or 1
+    lib = os.path.join(ROOT, "oracle", "_build", "libifc_oracle_omp.so")
+    env = dict(os.environ, IFC_ORACLE_LIB=lib, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="true")
+    cfg = workload_cfg()
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "time_port.py"), "--seconds", str(seconds),
+                        "--nx", str(cfg["nx"]), "--ny", str(cfg["ny"])],
+                       env=env, capture_output=True, text=True, timeout=seconds * 6 + 120)
+    if r.returncode != 0:
+        return {"error": (r.stderr or r.stdout)[-300:]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": d["cell_updates"] / d["seconds"], "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{d['outer_iterations']} outer iterations of {workload_name()} from rest, C oracle with "
+                      f"OpenMP row loops (FP32, red-black GS, gcc -O2), {d['seconds']:.1f} s on {threads} threads of "
+                      f"{host_cpu()}"}
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -299,8 +323,10 @@ def run_ours(args):
     upd_all, e2e_upd_all = tot.tolist()
 
     cpu = None
+    cpu_all = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_seconds)
+        cpu_all = cpu_baseline_all_cores(args.cpu_seconds)
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -333,6 +359,8 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if cpu_all:
+            line["cpu_baseline_all_cores"] = cpu_all
         if world == 1 and not args.no_forms and CONVECTION == "upwind":
             forms = {}
             for name, fn in (("precision", lambda: precision_summary(args.n3d)),

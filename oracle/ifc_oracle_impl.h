@@ -37,6 +37,20 @@ struct CAT(orc_state_, S) {
 static inline T CAT(min0_, S)(T x) { return x < (T)0 ? x : (T)0; }
 #define MIN0 CAT(min0_, S)
 
+/* OpenMP build (make -C oracle oracle_omp, for the all-cores CPU baseline
+ * only): the per-cell loops of the sweeps, the link coefficients and
+ * Rhie-Chow run over rows in parallel.  Each cell is computed as in the
+ * serial build; only the FP64 sums of the sweeps are added in another order. */
+#ifndef ORC_PAR_ROWS
+#ifdef ORC_OMP
+#define ORC_PAR_ROWS _Pragma("omp parallel for collapse(2) schedule(static)")
+#define ORC_PAR_ROWS_SUM _Pragma("omp parallel for collapse(2) schedule(static) reduction(+ : sq)")
+#else
+#define ORC_PAR_ROWS
+#define ORC_PAR_ROWS_SUM
+#endif
+#endif
+
 ST *FN(create)(const orc_config *cfg)
 {
     ST *s = (ST *)calloc(1, sizeof(ST));
@@ -163,6 +177,7 @@ void FN(mom_link_coef)(ST *s)
     T *a = s->f[ORC_F_MCOEF];
     const size_t N = s->N;
     const T rho = s->rho, mu = s->mu, Ax = s->Ax, Ay = s->Ay, Az = s->Az;
+    ORC_PAR_ROWS
     for (int k = 0; k < s->nz; ++k)
         for (int j = 0; j < s->ny; ++j)
             for (int i = 0; i < s->nx; ++i) {
@@ -419,11 +434,13 @@ double FN(sweep)(ST *s, int eq, int mode)
                 for (int i = 0; i < s->nx; ++i)
                     sq += CAT(point_update_, S)(s, s->tmp, phi, a, b, i, j, k, relax);
     } else if (mode == ORC_GS_REDBLACK) {
-        for (int color = 0; color < 2; ++color)
+        for (int color = 0; color < 2; ++color) {
+            ORC_PAR_ROWS_SUM
             for (int k = 0; k < s->nz; ++k)
                 for (int j = 0; j < s->ny; ++j)
                     for (int i = (color + j + k) & 1; i < s->nx; i += 2)
                         sq += CAT(point_update_, S)(s, phi, phi, a, b, i, j, k, relax);
+        }
     } else {
         for (int k = 0; k < s->nz; ++k)
             for (int j = 0; j < s->ny; ++j)
@@ -484,6 +501,7 @@ void FN(rhie_chow)(ST *s)
     const int cw = CAT(closed_face_, S)(s, ORC_WEST), ce = CAT(closed_face_, S)(s, ORC_EAST);
     const int cs = CAT(closed_face_, S)(s, ORC_SOUTH), cn = CAT(closed_face_, S)(s, ORC_NORTH);
     const int cb = CAT(closed_face_, S)(s, ORC_BOTTOM), ct = CAT(closed_face_, S)(s, ORC_TOP);
+    ORC_PAR_ROWS
     for (int k = 0; k < s->nz; ++k)
         for (int j = 0; j < s->ny; ++j)
             for (int i = 1; i < s->nx; ++i) {
@@ -493,6 +511,7 @@ void FN(rhie_chow)(ST *s)
                 T pRR = i <= s->nx - 2 ? p[R + 1] : (ce ? pR : (T)0);
                 uf[UFID(s, i, j, k)] = CAT(rc_face_, S)(u[L], u[R], a[L], a[R], pLL, pL, pR, pRR, s->Ax);
             }
+    ORC_PAR_ROWS
     for (int k = 0; k < s->nz; ++k)
         for (int j = 1; j < s->ny; ++j)
             for (int i = 0; i < s->nx; ++i) {
@@ -504,6 +523,7 @@ void FN(rhie_chow)(ST *s)
             }
     if (s->dim == 3) {
         size_t pl = (size_t)s->nx * s->ny;
+        ORC_PAR_ROWS
         for (int k = 1; k < s->nz; ++k)
             for (int j = 0; j < s->ny; ++j)
                 for (int i = 0; i < s->nx; ++i) {

@@ -18,7 +18,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libifc_oracle.so")
+# IFC_ORACLE_LIB selects another build of the same restatement (the OpenMP one,
+# _build/libifc_oracle_omp.so, times the all-cores CPU baseline).
+LIB_PATH = os.environ.get("IFC_ORACLE_LIB") or os.path.join(HERE, "_build", "libifc_oracle.so")
 
 GS_LEX, GS_REDBLACK, JACOBI = 0, 1, 2
 CRIT_REFERENCE, CRIT_PER_FIELD, CRIT_RESIDUAL = 0, 1, 2
@@ -59,7 +61,8 @@ class OrcNorms(C.Structure):
 def build(force: bool = False) -> str:
     """Compile the oracle with gcc (make -C oracle); returns the library path."""
     if force or not os.path.exists(LIB_PATH) or _stale():
-        subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+        target = "oracle_omp" if LIB_PATH.endswith("_omp.so") else "oracle"
+        subprocess.run(["make", "-s", "-C", HERE, target], check=True)
     return LIB_PATH
 
 

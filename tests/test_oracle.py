@@ -110,3 +110,35 @@ def test_residual_rule_restatement():
     o3.solve()
     for k in ("u", "v"):
         assert rel_l2(o2.field(k), o3.field(k)) < 1e-4, k
+
+
+def test_openmp_build_matches_the_serial_oracle(tmp_path):
+    """The OpenMP build of the oracle (the all-cores CPU baseline of bench.py)
+    computes every cell as the serial build does: after outer iterations with
+    every inner sweep run (no early exit), the fields are the same bits."""
+    import os
+    import subprocess
+    import sys
+
+    import ifc
+    from helpers import to_oracle_cfg
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"), "oracle_omp"], check=True)
+    cfg = dict(ifc.channel2d(48, 20, nIter_u=3, nIter_v=3, nIter_p=6), tol_u=0.0, tol_v=0.0, tol_p=0.0)
+    out = tmp_path / "omp.npz"
+    code = ("import sys, numpy as np; sys.path[:0] = %r; import ifc, oracle as O; from helpers import to_oracle_cfg; "
+            "o = O.Oracle(to_oracle_cfg(%r), 'f'); [o.outer_iteration() for _ in range(5)]; "
+            "np.savez(%r, **{k: o.field(k) for k in ('u', 'v', 'p', 'uf', 'vf')}); print(O.LIB_PATH)"
+            % ([os.path.join(root, "oracle"), os.path.join(root, "tests"),
+                os.path.join(root, "incompflow-cuda_b200", "python")], cfg, str(out)))
+    env = dict(os.environ, IFC_ORACLE_LIB=os.path.join(root, "oracle", "_build", "libifc_oracle_omp.so"),
+               OMP_NUM_THREADS="4")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "_omp.so" in r.stdout, r.stdout + r.stderr
+    o = O.Oracle(to_oracle_cfg(cfg), "f")
+    for _ in range(5):
+        o.outer_iteration()
+    got = np.load(out)
+    for k in ("u", "v", "p", "uf", "vf"):
+        np.testing.assert_array_equal(got[k], o.field(k), err_msg=k)
